@@ -1,0 +1,94 @@
+"""ctypes binding of libcuhc.so (built in-tree by cuhc_b200/build.py).
+
+The declarations mirror the C ABI in include/cuhc.h, which keeps the
+reference's eight entry points (shangar21/cuhc python/cuhc/_lib.py:19-91)
+unchanged and adds device-pointer variants and pass statistics. Importing
+fails loudly when the library is missing: there is no CPU fallback.
+"""
+
+import ctypes
+import pathlib
+
+_LIB_PATH = pathlib.Path(__file__).resolve().parent / "libcuhc.so"
+
+if not _LIB_PATH.exists():
+    raise ImportError(
+        f"{_LIB_PATH} is missing; build it with `python -m cuhc_b200.build` "
+        "(nvcc for sm_100a). cuhc_b200 has no CPU fallback.")
+
+lib = ctypes.CDLL(str(_LIB_PATH))
+
+_f32 = ctypes.POINTER(ctypes.c_float)
+_f64 = ctypes.POINTER(ctypes.c_double)
+_i64 = ctypes.POINTER(ctypes.c_int64)
+_u64 = ctypes.POINTER(ctypes.c_uint64)
+_int, _float = ctypes.c_int, ctypes.c_float
+
+lib.cuhc_pairwise_distances.restype = _int
+lib.cuhc_pairwise_distances.argtypes = [_f32, _int, _f32, _int, _int, _int, _float, _f32]
+lib.cuhc_linkage.restype = _int
+lib.cuhc_linkage.argtypes = [_f32, _int, _int, _int, _float, _int, _int, _f64]
+lib.cuhc_ward_rnn_with_options.restype = _int
+lib.cuhc_ward_rnn_with_options.argtypes = [_f32, _int, _int, _float, _int, _int, _f64]
+lib.cuhc_hdbscan_tree.restype = _int
+lib.cuhc_hdbscan_tree.argtypes = [_f32, _int, _int, _int, _float, _int, _float, _int, _f64, _f32]
+lib.cuhc_condense_tree.restype = ctypes.c_int64
+lib.cuhc_condense_tree.argtypes = [_f64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                   _i64, _i64, _f64, _i64]
+lib.cuhc_set_pruning.restype = _int
+lib.cuhc_set_pruning.argtypes = [_int]
+lib.cuhc_prune_stats.restype = None
+lib.cuhc_prune_stats.argtypes = [_u64, _u64]
+lib.cuhc_error_string.restype = ctypes.c_char_p
+lib.cuhc_error_string.argtypes = [_int]
+
+# Additions (no counterpart in the reference).
+lib.cuhc_linkage_device.restype = _int
+lib.cuhc_linkage_device.argtypes = [ctypes.c_void_p, _int, _int, _int, _float, _int, _int, _f64]
+lib.cuhc_hdbscan_tree_device.restype = _int
+lib.cuhc_hdbscan_tree_device.argtypes = [ctypes.c_void_p, _int, _int, _int, _float, _int, _float,
+                                         _int, _f64, _f32]
+lib.cuhc_pass_stats.restype = _int
+lib.cuhc_pass_stats.argtypes = [_u64, _int]
+
+PRUNE_MODES = {"auto": 0, "always": 1, "never": 2}
+# cudaErrorMemoryAllocation, reported by the dense path as MemoryError.
+CUDA_ERROR_OUT_OF_MEMORY = 2
+
+
+def check(status):
+    """RuntimeError with the library's message for a non-zero status."""
+    if status != 0:
+        raise RuntimeError(f"cuhc: {lib.cuhc_error_string(status).decode()} (code {status})")
+
+
+def float_ptr(array):
+    return array.ctypes.data_as(_f32)
+
+
+def double_ptr(array):
+    return array.ctypes.data_as(_f64)
+
+
+def int64_ptr(array):
+    return array.ctypes.data_as(_i64)
+
+
+def set_pruning(mode):
+    """Spatial pruning of the matrix-free paths: "auto", "always" or "never".
+    Results are identical in every mode; only the time changes."""
+    check(lib.cuhc_set_pruning(PRUNE_MODES[mode]))
+
+
+def prune_stats():
+    """(tiles computed, tiles in all passes) since the last call; resets."""
+    computed, total = ctypes.c_uint64(), ctypes.c_uint64()
+    lib.cuhc_prune_stats(ctypes.byref(computed), ctypes.byref(total))
+    return computed.value, total.value
+
+
+def pass_stats():
+    """Cumulative (tiles computed, tiles total, passes, Borůvka rounds)."""
+    out = (ctypes.c_uint64 * 4)()
+    lib.cuhc_pass_stats(out, 4)
+    return tuple(int(x) for x in out)

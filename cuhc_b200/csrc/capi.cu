@@ -1,0 +1,379 @@
+// The C ABI of libcuhc.so (declared in include/cuhc.h).
+//
+// The first eight functions are the reference's ctypes boundary
+// (capi.cu:133-366 of shangar21/cuhc) with the same names, signatures,
+// argument meaning, id tables, validation order and status codes, so the
+// reference's Python layer can load this library unchanged. Host pointers in,
+// host results out; device memory comes from the stream-ordered pool.
+//
+// The other functions are additions with no counterpart in the reference:
+// device-pointer variants (inputs already in HBM, for callers that keep data
+// on the GPU) and extended pass statistics.
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "mst.cuh"
+#include "metrics.cuh"
+#include "pairwise.cuh"
+#include "rnn.cuh"
+
+namespace cuhc {
+
+// Linkage ids (reference linkage.cuh:31) and algorithm ids (capi.cu:33-38).
+enum LinkageId : int { kSingle = 0, kComplete = 1, kAverage = 2, kWard = 3 };
+enum AlgorithmId : int { kDense = 0, kMst = 1, kNnChain = 2, kRnn = 3 };
+// Pruning modes of cuhc_set_pruning (reference spatial.cuh:354).
+enum PruneMode : int { kPruneAuto = 0, kPruneAlways = 1, kPruneNever = 2 };
+// Core-distance methods (reference hdbscan.cuh:324).
+enum CoreMethod : int { kCoreAuto = 0, kCoreFused = 1, kCoreRadix = 2 };
+constexpr int kMaxFusedK = 64;     // reference hdbscan.cuh:112
+constexpr int kMaxPruneFeatures = 256;
+// Largest k whose per-row lists fit in shared memory (128 rows x k floats).
+constexpr int kMaxListK = 256;
+
+std::atomic<int> gPruneMode{kPruneAuto};
+std::mutex gStatsMutex;
+PassStats gStats;
+
+void addStats(const PassStats &s) {
+  std::lock_guard<std::mutex> lock(gStatsMutex);
+  gStats.tilesComputed += s.tilesComputed;
+  gStats.tilesTotal += s.tilesTotal;
+  gStats.passes += s.passes;
+  gStats.rounds += s.rounds;
+}
+
+// Whether a call builds the k-d order and prunes with boxes. Results never
+// depend on it. "auto" prunes whenever the metric has a box bound: the GPU
+// k-d build costs about one pass of a small input, and the traversal is
+// nearly free when boxes separate nothing.
+template <class Metric> bool shouldPrune(int n, int d) {
+  const int mode = gPruneMode.load();
+  return Metric::kBoxBound && mode != kPruneNever && numTilesFor(n) >= 2 && d <= kMaxPruneFeatures;
+}
+
+// One stream per call, and a pool that keeps its memory between calls.
+struct CallContext {
+  cudaStream_t stream = nullptr;
+  int status = 0;
+  CallContext() {
+    static std::once_flag once;
+    std::call_once(once, [] {
+      int device = 0;
+      cudaGetDevice(&device);
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        unsigned long long threshold = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+      }
+    });
+    status = (int)cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+  }
+  ~CallContext() {
+    if (stream) {
+      cudaStreamSynchronize(stream);
+      cudaStreamDestroy(stream);
+    }
+  }
+};
+
+__global__ void scatterByOrder(const float *__restrict__ byPosition, const int *__restrict__ order,
+                               float *__restrict__ byOriginal, int n) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n)
+    byOriginal[order[p]] = byPosition[p];
+}
+
+// Single linkage by Borůvka on device points; tree to the host.
+template <class Metric>
+int singleLinkageMst(const float *devPoints, int n, int d, const Metric &m, double *hostTree,
+                     cudaStream_t s) {
+  StatusChain st;
+  SpatialIndex index;
+  const bool prune = shouldPrune<Metric>(n, d);
+  CUHC_TRY(st, index.build(devPoints, n, d, prune, s));
+  DeviceEdges edges;
+  PassStats stats;
+  CUHC_TRY(st, (boruvkaMst<Metric, PlainWeight>(index, m, PlainWeight{}, prune, edges, &stats, s)));
+  std::vector<int> u, v;
+  std::vector<float> w;
+  CUHC_TRY(st, sortEdgesToHost(edges, edges.count, s, u, v, w));
+  if (st.ok() && (int)u.size() != n - 1)
+    st(kErrorDisconnected);
+  if (st.ok())
+    treeFromOrderedMerges(u, v, w, n, hostTree);
+  addStats(stats);
+  return st.code;
+}
+
+template <class Metric>
+int hdbscanTree(const float *devPoints, int n, int d, const Metric &m, int minSamples, float alpha,
+                double *hostTree, float *hostCore, cudaStream_t s) {
+  StatusChain st;
+  SpatialIndex index;
+  const bool prune = shouldPrune<Metric>(n, d);
+  CUHC_TRY(st, index.build(devPoints, n, d, prune, s));
+  DeviceBuffer<float> core, coreOrig;
+  CUHC_TRY(st, core.allocate(n, s));
+  PassStats stats;
+  CUHC_TRY(st, coreDistances<Metric>(index, m, minSamples, prune, core.get(), &stats, s));
+  CUHC_TRY(st, index.updateMinValues(core.get()));
+  DeviceEdges edges;
+  MutualReachWeight weight;
+  weight.value = core.get();
+  weight.alpha = alpha;
+  if (n > 1)
+    CUHC_TRY(st, (boruvkaMst<Metric, MutualReachWeight>(index, m, weight, prune, edges, &stats, s)));
+  if (hostCore && st.ok()) {
+    CUHC_TRY(st, coreOrig.allocate(n, s));
+    scatterByOrder<<<(n + 255) / 256, 256, 0, s>>>(core.get(), index.order.get(), coreOrig.get(),
+                                                   n);
+    CUHC_TRY(st, cudaGetLastError());
+    CUHC_TRY(st, cudaMemcpyAsync(hostCore, coreOrig.get(), n * sizeof(float),
+                                 cudaMemcpyDeviceToHost, s));
+  }
+  if (n > 1) {
+    std::vector<int> u, v;
+    std::vector<float> w;
+    CUHC_TRY(st, sortEdgesToHost(edges, edges.count, s, u, v, w));
+    if (st.ok() && (int)u.size() != n - 1)
+      st(kErrorDisconnected);
+    if (st.ok())
+      treeFromOrderedMerges(u, v, w, n, hostTree);
+  }
+  CUHC_TRY(st, cudaStreamSynchronize(s));
+  addStats(stats);
+  return st.code;
+}
+
+int validateLinkage(int n, int d, int metricId, int linkageId, int algorithmId) {
+  if (n <= 0 || d <= 0)
+    return kErrorInvalidShape;
+  if (linkageId < kSingle || linkageId > kWard)
+    return kErrorInvalidLinkage;
+  const bool valid = algorithmId == kDense || (algorithmId == kMst && linkageId == kSingle) ||
+                     ((algorithmId == kNnChain || algorithmId == kRnn) && linkageId == kWard &&
+                      metricId == kEuclidean);
+  if (!valid)
+    return kErrorInvalidAlgorithm;
+  if (metricId < kEuclidean || metricId > kCosine)
+    return kErrorInvalidMetric;
+  return 0;
+}
+
+int linkageOnDevice(const float *devPoints, int n, int d, int metricId, float p, int linkageId,
+                    int algorithmId, double *hostTree, cudaStream_t s) {
+  if (algorithmId == kMst)
+    return withMetric(metricId, p, [&](auto m) {
+      return singleLinkageMst(devPoints, n, d, m, hostTree, s);
+    });
+  if (algorithmId == kRnn) {
+    RnnOptions options;
+    PassStats stats;
+    const int status = rnnWard(devPoints, n, d, options, hostTree, &stats, s);
+    addStats(stats);
+    return status;
+  }
+  if (algorithmId == kNnChain)
+    return nnChainWard(devPoints, n, d, hostTree, s);
+  return denseLinkage(devPoints, n, d, metricId, p, linkageId, hostTree, s);
+}
+
+int validateHdbscan(int n, int d, int minSamples, int coreMethod) {
+  if (n <= 0 || d <= 0 || minSamples < 1 || minSamples > n)
+    return kErrorInvalidShape;
+  if (coreMethod < 0 || coreMethod > 2 || (coreMethod == kCoreFused && minSamples > kMaxFusedK))
+    return kErrorInvalidAlgorithm;
+  if (minSamples > kMaxListK)
+    return kErrorTooLarge;
+  return 0;
+}
+
+} // namespace cuhc
+
+using namespace cuhc;
+
+extern "C" {
+
+int cuhc_pairwise_distances(const float *hostA, int nA, const float *hostB, int nB, int d,
+                            int metricId, float p, float *hostOut) {
+  if (nA <= 0 || nB <= 0 || d <= 0)
+    return kErrorInvalidShape;
+  if (metricId < kEuclidean || metricId > kCosine)
+    return kErrorInvalidMetric;
+  CallContext ctx;
+  StatusChain st;
+  st(ctx.status);
+  cudaStream_t s = ctx.stream;
+  DeviceBuffer<float> A, B, out;
+  CUHC_TRY(st, A.allocate((size_t)nA * d, s));
+  CUHC_TRY(st, out.allocate((size_t)nA * nB, s));
+  CUHC_TRY(st, cudaMemcpyAsync(A.get(), hostA, A.bytes(), cudaMemcpyHostToDevice, s));
+  if (hostB) {
+    CUHC_TRY(st, B.allocate((size_t)nB * d, s));
+    CUHC_TRY(st, cudaMemcpyAsync(B.get(), hostB, B.bytes(), cudaMemcpyHostToDevice, s));
+  }
+  if (st.ok())
+    st(withMetric(metricId, p, [&](auto m) {
+      return pairwiseDistances(A.get(), nA, hostB ? B.get() : nullptr, nB, d, m, out.get(), s);
+    }));
+  CUHC_TRY(st, cudaMemcpyAsync(hostOut, out.get(), out.bytes(), cudaMemcpyDeviceToHost, s));
+  CUHC_TRY(st, cudaStreamSynchronize(s));
+  return st.code;
+}
+
+int cuhc_linkage(const float *hostPoints, int n, int d, int metricId, float p, int linkageId,
+                 int algorithmId, double *hostTree) {
+  const int invalid = validateLinkage(n, d, metricId, linkageId, algorithmId);
+  if (invalid)
+    return invalid;
+  if (n == 1)
+    return 0;
+  CallContext ctx;
+  StatusChain st;
+  st(ctx.status);
+  DeviceBuffer<float> points;
+  CUHC_TRY(st, points.allocate((size_t)n * d, ctx.stream));
+  CUHC_TRY(st, cudaMemcpyAsync(points.get(), hostPoints, points.bytes(), cudaMemcpyHostToDevice,
+                               ctx.stream));
+  CUHC_TRY(st, linkageOnDevice(points.get(), n, d, metricId, p, linkageId, algorithmId, hostTree,
+                               ctx.stream));
+  return st.code;
+}
+
+int cuhc_ward_rnn_with_options(const float *hostPoints, int n, int d, float minProgress,
+                               int denseBelow, int allowDense, double *hostTree) {
+  if (n <= 0 || d <= 0)
+    return kErrorInvalidShape;
+  if (n == 1)
+    return 0;
+  CallContext ctx;
+  StatusChain st;
+  st(ctx.status);
+  DeviceBuffer<float> points;
+  CUHC_TRY(st, points.allocate((size_t)n * d, ctx.stream));
+  CUHC_TRY(st, cudaMemcpyAsync(points.get(), hostPoints, points.bytes(), cudaMemcpyHostToDevice,
+                               ctx.stream));
+  RnnOptions options;
+  options.minProgress = minProgress;
+  options.denseBelow = denseBelow;
+  options.allowDense = allowDense != 0;
+  PassStats stats;
+  CUHC_TRY(st, rnnWard(points.get(), n, d, options, hostTree, &stats, ctx.stream));
+  addStats(stats);
+  return st.code;
+}
+
+int cuhc_hdbscan_tree(const float *hostPoints, int n, int d, int metricId, float p,
+                      int minSamples, float alpha, int coreMethod, double *hostTree,
+                      float *hostCore) {
+  const int invalid = validateHdbscan(n, d, minSamples, coreMethod);
+  if (invalid)
+    return invalid;
+  if (metricId < kEuclidean || metricId > kCosine)
+    return kErrorInvalidMetric;
+  CallContext ctx;
+  StatusChain st;
+  st(ctx.status);
+  DeviceBuffer<float> points;
+  CUHC_TRY(st, points.allocate((size_t)n * d, ctx.stream));
+  CUHC_TRY(st, cudaMemcpyAsync(points.get(), hostPoints, points.bytes(), cudaMemcpyHostToDevice,
+                               ctx.stream));
+  if (st.ok())
+    st(withMetric(metricId, p, [&](auto m) {
+      return hdbscanTree(points.get(), n, d, m, minSamples, alpha, hostTree, hostCore, ctx.stream);
+    }));
+  return st.code;
+}
+
+long long cuhc_condense_tree(const double *tree, long long n, long long minClusterSize,
+                             long long capacity, long long *parent, long long *child,
+                             double *lambda, long long *size) {
+  return condenseTree(tree, n, minClusterSize, capacity, parent, child, lambda, size);
+}
+
+int cuhc_set_pruning(int mode) {
+  if (mode < kPruneAuto || mode > kPruneNever)
+    return kErrorInvalidAlgorithm;
+  gPruneMode.store(mode);
+  return 0;
+}
+
+void cuhc_prune_stats(unsigned long long *computed, unsigned long long *total) {
+  std::lock_guard<std::mutex> lock(gStatsMutex);
+  *computed = gStats.tilesComputed;
+  *total = gStats.tilesTotal;
+  gStats.tilesComputed = gStats.tilesTotal = 0;
+}
+
+const char *cuhc_error_string(int code) {
+  switch (code) {
+  case kErrorInvalidMetric:
+    return "invalid metric id";
+  case kErrorInvalidShape:
+    return "array dimensions must be positive";
+  case kErrorInvalidLinkage:
+    return "invalid linkage id";
+  case kErrorInvalidAlgorithm:
+    return "invalid algorithm id for this linkage";
+  case kErrorNonFinite:
+    return "distances overflowed float32 or are NaN; rescale the data";
+  case kErrorDisconnected:
+    return "some points have no finite distance to the others (NaN or infinite values?)";
+  case kErrorTimeout:
+    return "a device-side wait ran out of its iteration budget";
+  case kErrorTooLarge:
+    return "input exceeds a documented size limit of this entry point";
+  default:
+    return cudaGetErrorString((cudaError_t)code);
+  }
+}
+
+// ---- additions ------------------------------------------------------------
+
+int cuhc_linkage_device(const float *devicePoints, int n, int d, int metricId, float p,
+                        int linkageId, int algorithmId, double *hostTree) {
+  const int invalid = validateLinkage(n, d, metricId, linkageId, algorithmId);
+  if (invalid)
+    return invalid;
+  if (n == 1)
+    return 0;
+  CallContext ctx;
+  StatusChain st;
+  st(ctx.status);
+  CUHC_TRY(st, linkageOnDevice(devicePoints, n, d, metricId, p, linkageId, algorithmId, hostTree,
+                               ctx.stream));
+  return st.code;
+}
+
+int cuhc_hdbscan_tree_device(const float *devicePoints, int n, int d, int metricId, float p,
+                             int minSamples, float alpha, int coreMethod, double *hostTree,
+                             float *hostCore) {
+  const int invalid = validateHdbscan(n, d, minSamples, coreMethod);
+  if (invalid)
+    return invalid;
+  if (metricId < kEuclidean || metricId > kCosine)
+    return kErrorInvalidMetric;
+  CallContext ctx;
+  StatusChain st;
+  st(ctx.status);
+  if (st.ok())
+    st(withMetric(metricId, p, [&](auto m) {
+      return hdbscanTree(devicePoints, n, d, m, minSamples, alpha, hostTree, hostCore, ctx.stream);
+    }));
+  return st.code;
+}
+
+int cuhc_pass_stats(unsigned long long *out, int count) {
+  std::lock_guard<std::mutex> lock(gStatsMutex);
+  const unsigned long long values[4] = {gStats.tilesComputed, gStats.tilesTotal, gStats.passes,
+                                        gStats.rounds};
+  for (int i = 0; i < count && i < 4; ++i)
+    out[i] = values[i];
+  return 0;
+}
+
+} // extern "C"

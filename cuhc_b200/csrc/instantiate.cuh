@@ -1,0 +1,36 @@
+// Explicit instantiation of the per-metric entry points. One translation
+// unit per metric family (inst_*.cu) so that the builds run in parallel.
+#pragma once
+
+#include "boruvka.cuh"
+#include "pairwise.cuh"
+
+namespace cuhc {
+
+template <class Metric>
+int pairwiseDistances(const float *A, int nA, const float *B, int nB, int d, const Metric &m,
+                      float *out, cudaStream_t s) {
+  DeviceBuffer<float> tiledA, tiledB;
+  StatusChain st;
+  CUHC_TRY(st, buildTiled(A, nA, d, tiledA, s));
+  if (B)
+    CUHC_TRY(st, buildTiled(B, nB, d, tiledB, s));
+  CUHC_TRY(st, launchPairwise(tiledA.get(), B ? tiledB.get() : tiledA.get(), nA, nB, d, m, out, s));
+  CUHC_TRY(st, cudaStreamSynchronize(s));
+  return st.code;
+}
+
+} // namespace cuhc
+
+#define CUHC_INSTANTIATE_METRIC(M)                                                                 \
+  template int cuhc::boruvkaMst<M, cuhc::PlainWeight>(cuhc::SpatialIndex &, const M &,             \
+                                                      const cuhc::PlainWeight &, bool,             \
+                                                      cuhc::DeviceEdges &, cuhc::PassStats *,      \
+                                                      cudaStream_t);                               \
+  template int cuhc::boruvkaMst<M, cuhc::MutualReachWeight>(                                       \
+      cuhc::SpatialIndex &, const M &, const cuhc::MutualReachWeight &, bool, cuhc::DeviceEdges &, \
+      cuhc::PassStats *, cudaStream_t);                                                            \
+  template int cuhc::coreDistances<M>(cuhc::SpatialIndex &, const M &, int, bool, float *,         \
+                                      cuhc::PassStats *, cudaStream_t);                            \
+  template int cuhc::pairwiseDistances<M>(const float *, int, const float *, int, int, const M &,  \
+                                          float *, cudaStream_t);

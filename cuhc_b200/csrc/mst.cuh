@@ -1,0 +1,53 @@
+// Exact minimum spanning tree by Borůvka rounds, entirely on the GPU, and
+// the scipy-format merge tree built from it.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+#include "spatial.cuh"
+
+namespace cuhc {
+
+// Counters of the passes of one call (exported by cuhc_prune_stats and the
+// extended statistics call).
+struct PassStats {
+  unsigned long long tilesComputed = 0, tilesTotal = 0;
+  unsigned long long passes = 0, rounds = 0;
+};
+
+// MST edges in original point indices (u < v), on the device.
+struct DeviceEdges {
+  DeviceBuffer<int> u, v;
+  DeviceBuffer<float> w;
+  int count = 0;
+};
+
+// Sorts MST edges by the reference's edge order (weight, u, v)
+// (mst.cuh:41-48) on the device and copies them to the host.
+int sortEdgesToHost(DeviceEdges &edges, int numEdges, cudaStream_t stream, std::vector<int> &u,
+                    std::vector<int> &v, std::vector<float> &w);
+
+// scipy linkage rows from merges in tree order (each merge after the merges
+// that made its clusters): union-find names clusters, as the reference's
+// treeFromOrderedMerges (mst.cuh:204-228). Z receives (n-1) x 4 doubles.
+void treeFromOrderedMerges(const std::vector<int> &u, const std::vector<int> &v,
+                           const std::vector<float> &w, int n, double *Z);
+
+// Whether merges can form a tree: n-1 merges, finite heights, each joining
+// two clusters not yet joined (mst.cuh:188-202).
+bool mergesFormTree(const std::vector<int> &u, const std::vector<int> &v,
+                    const std::vector<float> &w, int n);
+
+// Borůvka over the points of an index (Metric x Weight instantiations in
+// boruvka_*.cu). Fills edges with the n-1 MST edges (original indices).
+template <class Metric, class Weight>
+int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, bool prune,
+               DeviceEdges &edges, PassStats *stats, cudaStream_t stream);
+
+// Exact core distances (k-th nearest, the point itself first) by position.
+template <class Metric>
+int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, float *core,
+                  PassStats *stats, cudaStream_t stream);
+
+} // namespace cuhc

@@ -1,0 +1,63 @@
+// Spatial index of a point set on the GPU: k-d order, tiled layout, BVH.
+//
+//  order     the k-d order: position p holds original point order[p]. Each
+//            range is split at a tile boundary near its middle (left side:
+//            floor(tiles / 2) tiles) along the feature with the widest
+//            spread of a sample, as the reference's spatialOrder does
+//            (spatial.cuh:44-91), but built on the GPU one tree level at a
+//            time with a radix sort per level instead of a CPU nth_element.
+//            Results never depend on the order: every pass breaks ties by
+//            original index.
+//  tiled     the points in HBM in the engine's layout: tile t, feature
+//            chunk c is a contiguous [KC][128] block (feature-major, zero
+//            padded), so one tile chunk is a single 16-byte-aligned copy of
+//            KC * 512 bytes straight into shared memory in the order the
+//            distance loop reads it.
+//  BVH       the balanced binary tree of the split: node = range of tiles,
+//            leaves = tiles. Every node has a bounding box; per pass each
+//            node also carries its smallest per-point value (core distance
+//            or cluster size) and its component if all its points share one.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace cuhc {
+
+struct BvhTopology {
+  int numNodes = 0, numTiles = 0, depth = 0;
+  // Host copies (breadth-first node order: parents before children, each
+  // level left to right, so every level is a contiguous node range).
+  std::vector<int> left, right, firstTile, tileCount, levelStart;
+  std::vector<int> leafOfTile;
+  void build(int numTiles);
+};
+
+struct SpatialIndex {
+  int n = 0, d = 0, numTiles = 0, kc = 0, numChunks = 0;
+  cudaStream_t stream = 0;
+  BvhTopology topo;
+  DeviceBuffer<float> tiled;         // numTiles * numChunks * kc * 128
+  DeviceBuffer<int> order, rank;     // position -> original, original -> position
+  DeviceBuffer<int> nodeLeft, nodeRight, nodeFirstTile, nodeTileCount, leafOfTile;
+  DeviceBuffer<float> nodeLow, nodeHigh; // numNodes * d
+  DeviceBuffer<float> nodeMinValue;      // numNodes
+  DeviceBuffer<int> nodePure;            // numNodes: component if pure, else -1
+  bool hasMinValues = false;             // nodeMinValue filled by updateMinValues
+
+  size_t tileFloats() const { return (size_t)numChunks * kc * kTile; }
+
+  // Builds everything from points (n x d row-major, original order, device).
+  // spatial=false keeps the original order (positions == original indices).
+  int build(const float *points, int n, int d, bool spatial, cudaStream_t stream);
+  // Re-tiles new point data already in position order (RNN centroids after a
+  // round), keeping the order arrays; recomputes boxes.
+  int retile(const float *pointsByPosition, int n);
+  // Per-node smallest value of values[position] (null: all zero).
+  int updateMinValues(const float *valuesByPosition);
+  // Per-node purity of component[position] (null: every node impure).
+  int updatePurity(const int *componentByPosition);
+};
+
+} // namespace cuhc

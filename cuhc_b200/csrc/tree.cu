@@ -1,0 +1,141 @@
+// Edge sorting on the device and merge-tree assembly on the host.
+#include "mst.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cub/device/device_radix_sort.cuh>
+#include <numeric>
+
+namespace cuhc {
+namespace {
+
+__global__ void edgeKeys(const int *__restrict__ u, const float *__restrict__ w,
+                         const int *__restrict__ perm, unsigned long long *__restrict__ keys,
+                         int m) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m)
+    return;
+  const int e = perm[i];
+  // Edge weights are >= 0 (clamped keys), so their bits order like floats.
+  keys[i] = ((unsigned long long)floatBits(w[e]) << 32) | (uint32_t)u[e];
+}
+
+__global__ void gatherEdges(const int *__restrict__ perm, const int *__restrict__ u,
+                            const int *__restrict__ v, const float *__restrict__ w,
+                            int *__restrict__ uo, int *__restrict__ vo, float *__restrict__ wo,
+                            int m) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m)
+    return;
+  const int e = perm[i];
+  uo[i] = u[e];
+  vo[i] = v[e];
+  wo[i] = w[e];
+}
+
+__global__ void iota(int *a, int m) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m)
+    a[i] = i;
+}
+
+} // namespace
+
+int sortEdgesToHost(DeviceEdges &edges, int m, cudaStream_t s, std::vector<int> &u,
+                    std::vector<int> &v, std::vector<float> &w) {
+  u.resize(m);
+  v.resize(m);
+  w.resize(m);
+  if (m == 0)
+    return 0;
+  StatusChain st;
+  DeviceBuffer<int> perm, perm2, vKeys, vKeysOut, uo, vo;
+  DeviceBuffer<float> wo;
+  DeviceBuffer<unsigned long long> keys, keysOut;
+  CUHC_TRY(st, perm.allocate(m, s));
+  CUHC_TRY(st, perm2.allocate(m, s));
+  CUHC_TRY(st, vKeysOut.allocate(m, s));
+  CUHC_TRY(st, keys.allocate(m, s));
+  CUHC_TRY(st, keysOut.allocate(m, s));
+  CUHC_TRY(st, uo.allocate(m, s));
+  CUHC_TRY(st, vo.allocate(m, s));
+  CUHC_TRY(st, wo.allocate(m, s));
+  if (!st.ok())
+    return st.code;
+  const int blocks = (m + 255) / 256;
+  iota<<<blocks, 256, 0, s>>>(perm.get(), m);
+  // Least significant key first: stable sort by v, then by (weight, u).
+  size_t t1 = 0, t2 = 0;
+  CUHC_TRY(st, cub::DeviceRadixSort::SortPairs(nullptr, t1, (const int *)edges.v.get(),
+                                               vKeysOut.get(), perm.get(), perm2.get(), m, 0, 32,
+                                               s));
+  CUHC_TRY(st, cub::DeviceRadixSort::SortPairs(nullptr, t2, keys.get(), keysOut.get(),
+                                               perm2.get(), perm.get(), m, 0, 64, s));
+  DeviceBuffer<unsigned char> temp;
+  CUHC_TRY(st, temp.allocate(std::max(t1, t2), s));
+  CUHC_TRY(st, cub::DeviceRadixSort::SortPairs(temp.get(), t1, (const int *)edges.v.get(),
+                                               vKeysOut.get(), perm.get(), perm2.get(), m, 0, 32,
+                                               s));
+  edgeKeys<<<blocks, 256, 0, s>>>(edges.u.get(), edges.w.get(), perm2.get(), keys.get(), m);
+  CUHC_TRY(st, cub::DeviceRadixSort::SortPairs(temp.get(), t2, keys.get(), keysOut.get(),
+                                               perm2.get(), perm.get(), m, 0, 64, s));
+  gatherEdges<<<blocks, 256, 0, s>>>(perm.get(), edges.u.get(), edges.v.get(), edges.w.get(),
+                                     uo.get(), vo.get(), wo.get(), m);
+  CUHC_TRY(st, cudaGetLastError());
+  CUHC_TRY(st, cudaMemcpyAsync(u.data(), uo.get(), m * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUHC_TRY(st, cudaMemcpyAsync(v.data(), vo.get(), m * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUHC_TRY(st, cudaMemcpyAsync(w.data(), wo.get(), m * sizeof(float), cudaMemcpyDeviceToHost, s));
+  CUHC_TRY(st, cudaStreamSynchronize(s));
+  return st.code;
+}
+
+namespace {
+inline int findRoot(std::vector<int> &parent, int x) {
+  while (parent[x] != x) {
+    parent[x] = parent[parent[x]];
+    x = parent[x];
+  }
+  return x;
+}
+} // namespace
+
+void treeFromOrderedMerges(const std::vector<int> &u, const std::vector<int> &v,
+                           const std::vector<float> &w, int n, double *Z) {
+  std::vector<int> parent(n), size(n, 1), id(n);
+  std::iota(parent.begin(), parent.end(), 0);
+  std::iota(id.begin(), id.end(), 0);
+  for (int s = 0; s < n - 1; ++s) {
+    int ru = findRoot(parent, u[s]), rv = findRoot(parent, v[s]);
+    const int a = id[ru], b = id[rv];
+    const int merged = size[ru] + size[rv];
+    double *row = Z + (size_t)s * 4;
+    row[0] = std::min(a, b);
+    row[1] = std::max(a, b);
+    row[2] = w[s];
+    row[3] = merged;
+    if (size[ru] < size[rv])
+      std::swap(ru, rv);
+    parent[rv] = ru;
+    size[ru] = merged;
+    id[ru] = n + s;
+  }
+}
+
+bool mergesFormTree(const std::vector<int> &u, const std::vector<int> &v,
+                    const std::vector<float> &w, int n) {
+  if ((int)u.size() != n - 1)
+    return false;
+  std::vector<int> parent(n);
+  std::iota(parent.begin(), parent.end(), 0);
+  for (int s = 0; s < n - 1; ++s) {
+    if (!std::isfinite(w[s]) || u[s] < 0 || u[s] >= n || v[s] < 0 || v[s] >= n)
+      return false;
+    const int ru = findRoot(parent, u[s]), rv = findRoot(parent, v[s]);
+    if (ru == rv)
+      return false;
+    parent[rv] = ru;
+  }
+  return true;
+}
+
+} // namespace cuhc
