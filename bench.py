@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""Benchmark of the exact HDBSCAN tree (1,000,000 x 8, min_samples 25).
+
+Workload: 20 isotropic Gaussian blobs (centres uniform in [-10, 10]^8,
+std 1.0, 45,000 points each) plus 100,000 points uniform over their bounding
+box, float32, shuffled, seed 1 -- synthetic data of the headline shape. One
+step = one full exact HDBSCAN single-linkage tree: core distances (k = 25),
+Borůvka MST of mutual reachability, sorted merges, scipy-format Z and the
+core distances copied to the host.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). `value` is the device-resident time per tree
+(points already in HBM, cuhc_hdbscan_tree_device); `e2e` is the same through
+the host API (cuhc_hdbscan_tree) with pinned host buffers, copies included.
+`--impl reference` runs the reference library (shangar21/cuhc built from its
+sources for sm_100a, oracle/_ref/libcuhc.so) through its own C ABI with host
+buffers and its default pruning, on the same data and GPU. With N > 1 GPUs
+each rank builds its own tree (replicas; the path does not shard).
+"""
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+METRIC = "1M-pt single/HDBSCAN MST time (s) on 1 B200, screened vs plain FP32, exact tree"
+UNIT = "s"
+N_POINTS, N_FEATURES, MIN_SAMPLES = 1_000_000, 8, 25
+L2_FLUSH_BYTES = 256 << 20
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def make_blobs_with_noise(seed=1, n=N_POINTS, d=N_FEATURES, centers=20, noise=0.10):
+    """The headline data set: equal Gaussian blobs (std 1) + uniform noise."""
+    rng = np.random.default_rng(seed)
+    n_noise = int(round(n * noise))
+    per = (n - n_noise) // centers
+    centres = rng.uniform(-10.0, 10.0, (centers, d))
+    pts = np.repeat(centres, per, axis=0) + rng.standard_normal((per * centers, d))
+    lo, hi = pts.min(axis=0), pts.max(axis=0)
+    X = np.vstack([pts, rng.uniform(lo, hi, (n - per * centers, d))]).astype(np.float32)
+    return np.ascontiguousarray(X[rng.permutation(len(X))])
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.proc, self.file = gpu, None, None
+
+    def __enter__(self):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.file:
+            return None
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        max_mhz = float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        loaded = sorted(sm)[len(sm) // 2:] if sm else []
+        return {"sm_mhz": float(np.median(loaded)) if loaded else None,
+                "sm_max_mhz": max_mhz, "reasons": reasons, "samples": len(rows)}
+
+
+def fp32_peak_tflops(torch):
+    """Measured FP32 (non-tensor) throughput: cuBLAS SGEMM 8192^3, TF32 off."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    a = torch.randn(8192, 8192, device="cuda")
+    b = torch.randn(8192, 8192, device="cuda")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = float("inf")
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        a @ b
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    return 2 * 8192 ** 3 / best / 1e12
+
+
+def measured_peaks():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def cpu_baseline(X):
+    """The CPU oracle (C restatement, OpenMP on every host core) timed on a
+    bounded sample: core distances of 6,000 rows against all points. A full
+    tree evaluates ~1.5 n^2 pairs (n^2 for the core distances, n^2 / 2 for
+    Prim's MST), so the sample's time per pair scales to the full workload."""
+    sys.path.insert(0, HERE)
+    from oracle import oracle as O  # noqa: PLC0415
+    rows = 6000
+    O.set_threads(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    O.core_distances(X, MIN_SAMPLES, rows=(0, rows))
+    elapsed = time.perf_counter() - t0
+    per_pair = elapsed / (rows * len(X))
+    full = 1.5 * len(X) ** 2 * per_pair
+    return {"value": round(full, 1), "unit": UNIT, "cores": O.threads(), "kind": "port",
+            "sample": f"core distances of {rows} rows x {len(X)} points in {elapsed:.1f} s, "
+                      f"scaled by 1.5 n^2 pairs per tree"}
+
+
+def run_reference(args, rank, world):
+    """The reference library on the same data, through its own C ABI."""
+    ref = os.path.join(HERE, "oracle", "_ref", "libcuhc.so")
+    config = {"workload": "hdbscan 1,000,000 x 8, 20 blobs + 10% noise, min_samples 25",
+              "n": N_POINTS, "d": N_FEATURES, "min_samples": MIN_SAMPLES, "pruning": "auto"}
+    if rank != 0:
+        return None
+    if not os.path.exists(ref):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libcuhc.so was not built "
+                "(the reference sources were absent when build() ran)"}
+    L = ctypes.CDLL(ref)
+    f32, f64 = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)
+    L.cuhc_hdbscan_tree.argtypes = [f32, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                    ctypes.c_int, ctypes.c_float, ctypes.c_int, f64, f32]
+    L.cuhc_set_pruning.argtypes = [ctypes.c_int]
+    X = make_blobs_with_noise()
+    tree = np.empty((len(X) - 1, 4), np.float64)
+    core = np.empty(len(X), np.float32)
+    L.cuhc_set_pruning(0)
+
+    def step():
+        status = L.cuhc_hdbscan_tree(X.ctypes.data_as(f32), len(X), X.shape[1], 0, 2.0,
+                                     MIN_SAMPLES, 1.0, 0, tree.ctypes.data_as(f64),
+                                     core.ctypes.data_as(f32))
+        if status != 0:
+            raise RuntimeError(f"reference status {status}")
+
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    value = float(np.mean(times))
+    return {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(value * 1e3, 2), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": 1,
+                             "kind": "reference",
+                             "sample": "the full workload: the reference library's host code "
+                                       "is single-threaded and its passes run on the GPU"}}
+
+
+def main():
+    parser = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    args = parser.parse_args()
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+
+    import torch  # plumbing: device buffers, events, process group  # noqa: PLC0415
+    import torch.distributed as dist  # noqa: PLC0415
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta  # noqa: PLC0415
+        dist.init_process_group("nccl", timeout=timedelta(minutes=5))
+
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    sys.path.insert(0, HERE)
+    from cuhc_b200 import _lib  # noqa: PLC0415
+
+    X = make_blobs_with_noise()
+    n, d = X.shape
+    f32, f64 = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)
+    X_dev = torch.from_numpy(X).cuda()
+    X_pin = torch.from_numpy(X).pin_memory()
+    tree_pin = torch.empty((n - 1) * 4, dtype=torch.float64).pin_memory()
+    core_pin = torch.empty(n, dtype=torch.float32).pin_memory()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    tree_ptr = ctypes.cast(tree_pin.data_ptr(), f64)
+    core_ptr = ctypes.cast(core_pin.data_ptr(), f32)
+
+    def device_step():
+        _lib.check(_lib.lib.cuhc_hdbscan_tree_device(
+            ctypes.c_void_p(X_dev.data_ptr()), n, d, 0, 2.0, MIN_SAMPLES, 1.0, 0, tree_ptr,
+            core_ptr))
+
+    def host_step():
+        _lib.check(_lib.lib.cuhc_hdbscan_tree(
+            ctypes.cast(X_pin.data_ptr(), f32), n, d, 0, 2.0, MIN_SAMPLES, 1.0, 0, tree_ptr,
+            core_ptr))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def timed(step, k):
+        """Device time per step (CUDA events; L2 flushed before each step)."""
+        times = []
+        for _ in range(k):
+            flush.zero_()
+            torch.cuda.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            step()
+            e.record()
+            e.synchronize()
+            times.append(s.elapsed_time(e) / 1e3)
+        return times
+
+    for _ in range(args.warmup):
+        device_step()
+    barrier()
+    launches0 = _lib.launch_count()
+    stats0 = _lib.pass_stats()
+    with ClockSampler(local_rank) as clocks:
+        barrier()
+        times = timed(device_step, args.steps)
+        barrier()
+    launches = (_lib.launch_count() - launches0) // max(args.steps, 1)
+    stats1 = _lib.pass_stats()
+    per_step = float(np.mean(times))
+
+    # Kernel-level figures: the pass kernels timed on their own stream.
+    _lib.set_timing(True)
+    _lib.kernel_timing()
+    timed(device_step, 1)
+    kt = _lib.kernel_timing()
+    _lib.set_timing(False)
+
+    # End to end through the host API (pinned buffers, copies included).
+    for _ in range(1):
+        host_step()
+    e2e_times = timed(host_step, args.steps)
+    e2e = float(np.mean(e2e_times))
+
+    # Max over ranks.
+    t = torch.tensor([per_step, e2e], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    per_step, e2e = float(t[0]), float(t[1])
+
+    if rank == 0:
+        peaks, peak_kind = measured_peaks()
+        fp32 = fp32_peak_tflops(torch)
+        knn_ms, knn_launch, knn_tiles = kt["knn_pass"]
+        near_ms, near_launch, near_tiles = kt["nearest_pass"]
+        # Dominant kernel: the pass kind with the most device time. Work per
+        # evaluated pair: 3 d FP32 FLOP (d subtractions + d fused multiply-adds).
+        kind, (ms, nl, tiles) = max(kt.items(), key=lambda kv: kv[1][0])
+        flops = tiles * 128 * 128 * 3 * d
+        achieved = flops / (ms / 1e3) / 1e12 if ms > 0 else 0.0
+        line = {
+            "metric": METRIC, "value": round(per_step, 4), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 2),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "hdbscan 1,000,000 x 8, 20 blobs + 10% noise, min_samples 25",
+                       "n": n, "d": d, "min_samples": MIN_SAMPLES, "path": "plain exact fp32",
+                       "l2": "flushed before every step (256 MB write)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": int(X.nbytes),
+                    "d2h_bytes_per_step": int((n - 1) * 4 * 8 + n * 4)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "fp32", "kernel": kind, "achieved": round(achieved, 2),
+                         "peak": round(fp32, 2), "unit": "TFLOP/s",
+                         "frac": round(achieved / fp32, 3) if fp32 else None,
+                         "traffic": None,
+                         "peak_source": "cuBLAS SGEMM 8192^3 with TF32 off, measured in this run "
+                                        "(the plain pass runs on the FP32 pipe); "
+                                        f"bf16 tensor peak {peaks.get('bf16_tflops')} TFLOP/s "
+                                        f"({peak_kind})",
+                         "work": f"{tiles} tiles x 16384 pairs x 3d FLOP in {nl} launches, "
+                                 f"{ms:.1f} ms"},
+            "passes": {"knn": {"ms": round(knn_ms, 2), "launches": knn_launch,
+                               "tiles": knn_tiles},
+                       "nearest": {"ms": round(near_ms, 2), "launches": near_launch,
+                                   "tiles": near_tiles},
+                       "tiles_per_step": int((stats1[0] - stats0[0]) / max(args.steps, 1)),
+                       "rounds_per_step": (stats1[3] - stats0[3]) / max(args.steps, 1)},
+            "clocks": clocks.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(X)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -51,7 +51,19 @@ lib.cuhc_hdbscan_tree_device.argtypes = [ctypes.c_void_p, _int, _int, _int, _flo
 lib.cuhc_pass_stats.restype = _int
 lib.cuhc_pass_stats.argtypes = [_u64, _int]
 
+lib.cuhc_hdbscan_labels.restype = _int
+lib.cuhc_hdbscan_labels.argtypes = [_f64, ctypes.c_int64, ctypes.c_int64, _int, _int,
+                                    ctypes.c_double, ctypes.c_int64, _i64, _f64]
+lib.cuhc_launch_count.restype = ctypes.c_uint64
+lib.cuhc_launch_count.argtypes = []
+lib.cuhc_set_timing.restype = _int
+lib.cuhc_set_timing.argtypes = [_int]
+lib.cuhc_kernel_timing.restype = _int
+lib.cuhc_kernel_timing.argtypes = [_f64, _u64, _u64, _int]
+
 PRUNE_MODES = {"auto": 0, "always": 1, "never": 2}
+# Pass kinds of cuhc_kernel_timing.
+TIMER_KINDS = ("knn_pass", "nearest_pass", "screen_pass", "reserved")
 # cudaErrorMemoryAllocation, reported by the dense path as MemoryError.
 CUDA_ERROR_OUT_OF_MEMORY = 2
 
@@ -92,3 +104,21 @@ def pass_stats():
     out = (ctypes.c_uint64 * 4)()
     lib.cuhc_pass_stats(out, 4)
     return tuple(int(x) for x in out)
+
+
+def launch_count():
+    """Kernel launches of libcuhc.so since it was loaded."""
+    return int(lib.cuhc_launch_count())
+
+
+def set_timing(on):
+    """Per-pass CUDA-event timing on the launching stream (off by default)."""
+    check(lib.cuhc_set_timing(1 if on else 0))
+
+
+def kernel_timing():
+    """{kind: (device ms, launches, tiles computed)} since the last call; resets."""
+    ms = (ctypes.c_double * 4)()
+    launches, tiles = (ctypes.c_uint64 * 4)(), (ctypes.c_uint64 * 4)()
+    check(lib.cuhc_kernel_timing(ms, launches, tiles, 4))
+    return {TIMER_KINDS[i]: (ms[i], int(launches[i]), int(tiles[i])) for i in range(4)}

@@ -22,6 +22,7 @@
 
 #include <algorithm>
 
+#include "profiling.cuh"
 #include "mst.cuh"
 #include "passes.cuh"
 
@@ -175,7 +176,7 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
   CUHC_TRY(st, compV.allocate(n, stream));
   if (!st.ok())
     return st.code;
-  iotaKernel<<<blocks(n), 256, 0, stream>>>(comp.get(), n);
+  iotaKernel<<<blocks(n), 256, 0, stream>>>(comp.get(), n); noteLaunch();
   CUHC_TRY(st, cudaMemsetAsync(nearest.get(), 0xff, n * sizeof(unsigned long long), stream));
   CUHC_TRY(st, cudaMemsetAsync(error.get(), 0, sizeof(int), stream));
   CUHC_TRY(st, cudaMemsetAsync(tiles.get(), 0, sizeof(unsigned long long), stream));
@@ -203,33 +204,47 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
   p.error = error.get();
 
   int numComponents = n, totalEdges = 0, rounds = 0;
+  unsigned long long tilesSoFar = 0;
   int hostCounters[4];
   while (st.ok() && numComponents > 1) {
     CUHC_TRY(st, index.updatePurity(comp.get()));
-    fillU32<<<blocks(n), 256, 0, stream>>>(compBest.get(), 0x7f800000u, n);
-    if (rounds > 0)
+    fillU32<<<blocks(n), 256, 0, stream>>>(compBest.get(), 0x7f800000u, n); noteLaunch();
+    if (rounds > 0) {
       seedComponentBest<<<blocks(n), 256, 0, stream>>>(nearest.get(), index.rank.get(),
                                                        comp.get(), compBest.get(), n);
+      noteLaunch();
+    }
     CUHC_TRY(st, cudaGetLastError());
-    CUHC_TRY(st, (launchPass<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
+    {
+      PassTimer timer(kTimerNearestPass, stream);
+      CUHC_TRY(st, (launchPass<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
+      if (timer.start) {
+        unsigned long long tilesNow = 0;
+        cudaMemcpyAsync(&tilesNow, tiles.get(), sizeof(tilesNow), cudaMemcpyDeviceToHost, stream);
+        timer.finish(tilesNow - tilesSoFar);
+        tilesSoFar = tilesNow;
+      }
+    }
     CUHC_TRY(st, cudaMemsetAsync(compKey.get(), 0xff, n * sizeof(unsigned long long), stream));
     CUHC_TRY(st, cudaMemsetAsync(compV.get(), 0xff, n * sizeof(unsigned int), stream));
     CUHC_TRY(st, cudaMemsetAsync(counters.get(), 0, 4 * sizeof(int), stream));
     componentKeyPass1<<<blocks(n), 256, 0, stream>>>(nearest.get(), index.order.get(), comp.get(),
-                                                     compKey.get(), n);
+                                                     compKey.get(), n); noteLaunch();
     componentKeyPass2<<<blocks(n), 256, 0, stream>>>(nearest.get(), index.order.get(), comp.get(),
-                                                     compKey.get(), compV.get(), n);
+                                                     compKey.get(), compV.get(), n); noteLaunch();
     hookComponents<<<blocks(n), 256, 0, stream>>>(
         comp.get(), index.rank.get(), compKey.get(), compV.get(), parent.get(),
         edges.u.get() + totalEdges, edges.v.get() + totalEdges, edges.w.get() + totalEdges,
-        counters.get(), n - 1 - totalEdges, n);
+        counters.get(), n - 1 - totalEdges, n); noteLaunch();
     int jumps = 1;
     while ((1 << jumps) < numComponents)
       ++jumps;
-    for (int j = 0; j <= jumps; ++j)
+    for (int j = 0; j <= jumps; ++j) {
       jumpParents<<<blocks(n), 256, 0, stream>>>(comp.get(), parent.get(), n);
-    countRoots<<<blocks(n), 256, 0, stream>>>(comp.get(), parent.get(), counters.get(), n);
-    relabel<<<blocks(n), 256, 0, stream>>>(comp.get(), parent.get(), n);
+      noteLaunch();
+    }
+    countRoots<<<blocks(n), 256, 0, stream>>>(comp.get(), parent.get(), counters.get(), n); noteLaunch();
+    relabel<<<blocks(n), 256, 0, stream>>>(comp.get(), parent.get(), n); noteLaunch();
     CUHC_TRY(st, cudaGetLastError());
     CUHC_TRY(st, cudaMemcpyAsync(hostCounters, counters.get(), 4 * sizeof(int),
                                  cudaMemcpyDeviceToHost, stream));
@@ -304,7 +319,16 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
   p.k = k;
   p.tilesComputed = tiles.get();
   p.error = error.get();
-  CUHC_TRY(st, (launchPass<Metric, PlainWeight, true>(p, metric, PlainWeight{}, index.kc, stream)));
+  {
+    PassTimer timer(kTimerKnnPass, stream);
+    CUHC_TRY(st,
+             (launchPass<Metric, PlainWeight, true>(p, metric, PlainWeight{}, index.kc, stream)));
+    if (timer.start) {
+      unsigned long long tilesNow = 0;
+      cudaMemcpyAsync(&tilesNow, tiles.get(), sizeof(tilesNow), cudaMemcpyDeviceToHost, stream);
+      timer.finish(tilesNow);
+    }
+  }
   int err = 0;
   unsigned long long tileCount = 0;
   CUHC_TRY(st, cudaMemcpyAsync(&err, error.get(), sizeof(int), cudaMemcpyDeviceToHost, stream));

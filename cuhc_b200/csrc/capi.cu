@@ -15,6 +15,7 @@
 #include <mutex>
 #include <vector>
 
+#include "profiling.cuh"
 #include "mst.cuh"
 #include "metrics.cuh"
 #include "pairwise.cuh"
@@ -37,6 +38,15 @@ constexpr int kMaxListK = 256;
 std::atomic<int> gPruneMode{kPruneAuto};
 std::mutex gStatsMutex;
 PassStats gStats;
+
+int currentPruneMode() { return gPruneMode.load(); }
+
+int pairwiseIntoMatrix(const float *points, int n, int d, int metricId, float p, float *out,
+                       cudaStream_t s) {
+  return withMetric(metricId, p, [&](auto m) {
+    return pairwiseDistances(points, n, nullptr, n, d, m, out, s);
+  });
+}
 
 void addStats(const PassStats &s) {
   std::lock_guard<std::mutex> lock(gStatsMutex);
@@ -130,7 +140,7 @@ int hdbscanTree(const float *devPoints, int n, int d, const Metric &m, int minSa
   if (hostCore && st.ok()) {
     CUHC_TRY(st, coreOrig.allocate(n, s));
     scatterByOrder<<<(n + 255) / 256, 256, 0, s>>>(core.get(), index.order.get(), coreOrig.get(),
-                                                   n);
+                                                   n); noteLaunch();
     CUHC_TRY(st, cudaGetLastError());
     CUHC_TRY(st, cudaMemcpyAsync(hostCore, coreOrig.get(), n * sizeof(float),
                                  cudaMemcpyDeviceToHost, s));

@@ -4,6 +4,7 @@
 // pairwiseDistanceKernel (distance_matrix.cuh:177-200) bit for bit.
 #pragma once
 
+#include "profiling.cuh"
 #include "engine.cuh"
 
 namespace cuhc {
@@ -45,16 +46,16 @@ int launchPairwise(const float *tiledA, const float *tiledB, int nA, int nB, int
   const size_t dyn = 2 * (size_t)kc * kTile * sizeof(float);
   switch (kc) {
   case 4:
-    pairwiseKernel<Metric, 4><<<grid, kThreads, dyn, s>>>(tiledA, tiledB, nA, nB, numChunks, m, out);
+    pairwiseKernel<Metric, 4><<<grid, kThreads, dyn, s>>>(tiledA, tiledB, nA, nB, numChunks, m, out); noteLaunch();
     break;
   case 8:
-    pairwiseKernel<Metric, 8><<<grid, kThreads, dyn, s>>>(tiledA, tiledB, nA, nB, numChunks, m, out);
+    pairwiseKernel<Metric, 8><<<grid, kThreads, dyn, s>>>(tiledA, tiledB, nA, nB, numChunks, m, out); noteLaunch();
     break;
   case 16:
-    pairwiseKernel<Metric, 16><<<grid, kThreads, dyn, s>>>(tiledA, tiledB, nA, nB, numChunks, m, out);
+    pairwiseKernel<Metric, 16><<<grid, kThreads, dyn, s>>>(tiledA, tiledB, nA, nB, numChunks, m, out); noteLaunch();
     break;
   default:
-    pairwiseKernel<Metric, 32><<<grid, kThreads, dyn, s>>>(tiledA, tiledB, nA, nB, numChunks, m, out);
+    pairwiseKernel<Metric, 32><<<grid, kThreads, dyn, s>>>(tiledA, tiledB, nA, nB, numChunks, m, out); noteLaunch();
     break;
   }
   return (int)cudaGetLastError();

@@ -16,6 +16,7 @@
 //                      (hdbscan.cuh:144-258).
 #pragma once
 
+#include "profiling.cuh"
 #include "engine.cuh"
 
 namespace cuhc {
@@ -302,7 +303,7 @@ int launchPass(const PassParams &p, const Metric &m, const Weight &w, int kc,
       if (e != cudaSuccess)
         return (int)e;
     }
-    kernel<<<p.numTiles, kThreads, dynBytes, stream>>>(p, m, w);
+    kernel<<<p.numTiles, kThreads, dynBytes, stream>>>(p, m, w); noteLaunch();
     return (int)cudaGetLastError();
   };
   switch (kc) {

@@ -27,6 +27,9 @@ int nnChainWard(const float *devPoints, int n, int d, double *hostTree, cudaStre
 int denseLinkage(const float *devPoints, int n, int d, int metricId, float p, int linkageId,
                  double *hostTree, cudaStream_t stream);
 
+// The pruning mode set by cuhc_set_pruning (0 auto, 1 always, 2 never).
+int currentPruneMode();
+
 // HDBSCAN's condensed tree of a (n-1) x 4 single-linkage tree (host):
 // rows in sklearn 1.9's order; returns the row count, or -(rows needed) if
 // capacity is too small.

@@ -1,4 +1,5 @@
 // GPU k-d ordering, tiled layout and BVH summaries (see spatial.cuh).
+#include "profiling.cuh"
 #include "spatial.cuh"
 
 #include <algorithm>
@@ -289,7 +290,7 @@ int SpatialIndex::build(const float *points, int n_, int d_, bool spatial, cudaS
                                cudaMemcpyHostToDevice, s));
   CUHC_TRY(st, cudaMemcpyAsync(leafOfTile.get(), topo.leafOfTile.data(), numTiles * sizeof(int),
                                cudaMemcpyHostToDevice, s));
-  iotaKernel<<<blocksFor(n, 256), 256, 0, s>>>(order.get(), n);
+  iotaKernel<<<blocksFor(n, 256), 256, 0, s>>>(order.get(), n); noteLaunch();
   CUHC_TRY(st, cudaGetLastError());
 
   if (spatial && topo.depth > 1 && st.ok()) {
@@ -313,10 +314,10 @@ int SpatialIndex::build(const float *points, int n_, int d_, bool spatial, cudaS
       const int lb = topo.levelStart[level], le = topo.levelStart[level + 1];
       chooseSplitKernel<<<blocksFor((long long)(le - lb) * 32, 256), 256, 0, s>>>(
           points, n, d, order.get(), nodeFirstTile.get(), nodeTileCount.get(), lb, le,
-          split.get());
+          split.get()); noteLaunch();
       levelKeysKernel<<<blocksFor(n, 256), 256, 0, s>>>(
           points, n, d, level, order.get(), nodeLeft.get(), nodeRight.get(), nodeFirstTile.get(),
-          nodeTileCount.get(), split.get(), keys.get());
+          nodeTileCount.get(), split.get(), keys.get()); noteLaunch();
       CUHC_TRY(st, cudaGetLastError());
       CUHC_TRY(st, cub::DeviceRadixSort::SortPairs(temp.get(), tempBytes, keys.get(),
                                                    keysOut.get(), order.get(), valsOut.get(), n,
@@ -329,7 +330,7 @@ int SpatialIndex::build(const float *points, int n_, int d_, bool spatial, cudaS
     return st.code;
   CUHC_TRY(st, cudaMemsetAsync(tiled.get(), 0, tiled.bytes(), s));
   gatherTiledKernel<<<blocksFor(n, 128), 128, 0, s>>>(points, n, d, kc, numChunks, order.get(),
-                                                      tiled.get(), rank.get());
+                                                      tiled.get(), rank.get()); noteLaunch();
   CUHC_TRY(st, cudaGetLastError());
   CUHC_TRY(st, retile(nullptr, n));
   return st.code;
@@ -357,17 +358,17 @@ int SpatialIndex::retile(const float *pointsByPosition, int newN) {
                                  stream));
     gatherTiledKernel<<<blocksFor(n, 128), 128, 0, stream>>>(pointsByPosition, n, d, kc,
                                                              numChunks, nullptr, tiled.get(),
-                                                             nullptr);
+                                                             nullptr); noteLaunch();
     CUHC_TRY(st, cudaGetLastError());
   }
   const int N = topo.numNodes;
   leafBoxKernel<<<blocksFor((long long)numTiles * 32, 128), 128, 0, stream>>>(
       tiled.get(), n, d, kc, numChunks, numTiles, leafOfTile.get(), nodeLow.get(),
-      nodeHigh.get());
+      nodeHigh.get()); noteLaunch();
   for (int level = topo.depth - 1; level >= 0; --level) {
     const int lb = topo.levelStart[level], le = topo.levelStart[level + 1];
     internalBoxKernel<<<blocksFor((long long)(le - lb) * d, 256), 256, 0, stream>>>(
-        lb, le, d, nodeLeft.get(), nodeRight.get(), nodeLow.get(), nodeHigh.get());
+        lb, le, d, nodeLeft.get(), nodeRight.get(), nodeLow.get(), nodeHigh.get()); noteLaunch();
   }
   (void)N;
   CUHC_TRY(st, cudaGetLastError());
@@ -377,22 +378,22 @@ int SpatialIndex::retile(const float *pointsByPosition, int newN) {
 int SpatialIndex::updateMinValues(const float *values) {
   hasMinValues = values != nullptr;
   leafSummaryKernel<<<blocksFor((long long)numTiles * 32, 128), 128, 0, stream>>>(
-      n, numTiles, leafOfTile.get(), values, nullptr, nodeMinValue.get(), nullptr);
+      n, numTiles, leafOfTile.get(), values, nullptr, nodeMinValue.get(), nullptr); noteLaunch();
   for (int level = topo.depth - 1; level >= 0; --level) {
     const int lb = topo.levelStart[level], le = topo.levelStart[level + 1];
     internalSummaryKernel<<<blocksFor(le - lb, 128), 128, 0, stream>>>(
-        lb, le, nodeLeft.get(), nodeRight.get(), nodeMinValue.get(), nullptr);
+        lb, le, nodeLeft.get(), nodeRight.get(), nodeMinValue.get(), nullptr); noteLaunch();
   }
   return (int)cudaGetLastError();
 }
 
 int SpatialIndex::updatePurity(const int *component) {
   leafSummaryKernel<<<blocksFor((long long)numTiles * 32, 128), 128, 0, stream>>>(
-      n, numTiles, leafOfTile.get(), nullptr, component, nullptr, nodePure.get());
+      n, numTiles, leafOfTile.get(), nullptr, component, nullptr, nodePure.get()); noteLaunch();
   for (int level = topo.depth - 1; level >= 0; --level) {
     const int lb = topo.levelStart[level], le = topo.levelStart[level + 1];
     internalSummaryKernel<<<blocksFor(le - lb, 128), 128, 0, stream>>>(
-        lb, le, nodeLeft.get(), nodeRight.get(), nullptr, nodePure.get());
+        lb, le, nodeLeft.get(), nodeRight.get(), nullptr, nodePure.get()); noteLaunch();
   }
   return (int)cudaGetLastError();
 }
@@ -409,7 +410,7 @@ int buildTiled(const float *points, int n, int d, DeviceBuffer<float> &tiled, cu
   if (!st.ok())
     return st.code;
   gatherTiledKernel<<<(n + 127) / 128, 128, 0, s>>>(points, n, d, kc, numChunks, nullptr,
-                                                    tiled.get(), nullptr);
+                                                    tiled.get(), nullptr); noteLaunch();
   CUHC_TRY(st, cudaGetLastError());
   return st.code;
 }

@@ -1,4 +1,5 @@
 // Edge sorting on the device and merge-tree assembly on the host.
+#include "profiling.cuh"
 #include "mst.cuh"
 
 #include <algorithm>
@@ -63,7 +64,7 @@ int sortEdgesToHost(DeviceEdges &edges, int m, cudaStream_t s, std::vector<int> 
   if (!st.ok())
     return st.code;
   const int blocks = (m + 255) / 256;
-  iota<<<blocks, 256, 0, s>>>(perm.get(), m);
+  iota<<<blocks, 256, 0, s>>>(perm.get(), m); noteLaunch();
   // Least significant key first: stable sort by v, then by (weight, u).
   size_t t1 = 0, t2 = 0;
   CUHC_TRY(st, cub::DeviceRadixSort::SortPairs(nullptr, t1, (const int *)edges.v.get(),
@@ -76,11 +77,11 @@ int sortEdgesToHost(DeviceEdges &edges, int m, cudaStream_t s, std::vector<int> 
   CUHC_TRY(st, cub::DeviceRadixSort::SortPairs(temp.get(), t1, (const int *)edges.v.get(),
                                                vKeysOut.get(), perm.get(), perm2.get(), m, 0, 32,
                                                s));
-  edgeKeys<<<blocks, 256, 0, s>>>(edges.u.get(), edges.w.get(), perm2.get(), keys.get(), m);
+  edgeKeys<<<blocks, 256, 0, s>>>(edges.u.get(), edges.w.get(), perm2.get(), keys.get(), m); noteLaunch();
   CUHC_TRY(st, cub::DeviceRadixSort::SortPairs(temp.get(), t2, keys.get(), keysOut.get(),
                                                perm2.get(), perm.get(), m, 0, 64, s));
   gatherEdges<<<blocks, 256, 0, s>>>(perm.get(), edges.u.get(), edges.v.get(), edges.w.get(),
-                                     uo.get(), vo.get(), wo.get(), m);
+                                     uo.get(), vo.get(), wo.get(), m); noteLaunch();
   CUHC_TRY(st, cudaGetLastError());
   CUHC_TRY(st, cudaMemcpyAsync(u.data(), uo.get(), m * sizeof(int), cudaMemcpyDeviceToHost, s));
   CUHC_TRY(st, cudaMemcpyAsync(v.data(), vo.get(), m * sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -1,0 +1,120 @@
+/*
+ * cuhc.h — C ABI of libcuhc.so (cuhc_b200), the drop-in boundary of the
+ * exact-clustering hot path of shangar21/cuhc.
+ *
+ * The first eight functions replace the reference's ctypes boundary one for
+ * one: same symbol names, signatures, argument meaning, id tables and status
+ * codes (reference src/capi.cu, bound by its python/cuhc/_lib.py:19-91). A
+ * ctypes caller of the reference library can load this one instead.
+ *
+ * Conventions (as in the reference):
+ *   - every pointer is HOST memory owned by the caller, except the *_device
+ *     additions, whose point arrays are DEVICE memory on the current device;
+ *   - points are row-major float32 (numPoints x numFeatures);
+ *   - calls are synchronous; device memory comes from a stream-ordered pool;
+ *   - status: 0 success, a positive cudaError_t, or a negative code below.
+ *
+ * Id tables:
+ *   metric     euclidean 0, sqeuclidean 1, manhattan 2, chebyshev 3,
+ *              minkowski 4 (order p), cosine 5         (reference capi.cu:17-24)
+ *   linkage    single 0, complete 1, average 2, ward 3 (reference linkage.cuh:31)
+ *   algorithm  dense 0, mst 1, nn_chain 2, rnn 3       (reference capi.cu:33-38)
+ *   coreMethod auto 0, fused 1, radix 2                (reference hdbscan.cuh:324)
+ *   pruning    auto 0, always 1, never 2               (reference spatial.cuh:354)
+ */
+#ifndef CUHC_B200_CUHC_H
+#define CUHC_B200_CUHC_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Negative status codes; -1..-6 are the reference's (capi.cu:26-30, mst.cuh:80-81). */
+#define CUHC_ERROR_INVALID_METRIC (-1)
+#define CUHC_ERROR_INVALID_SHAPE (-2)
+#define CUHC_ERROR_INVALID_LINKAGE (-3)
+#define CUHC_ERROR_INVALID_ALGORITHM (-4)
+#define CUHC_ERROR_DISCONNECTED (-5)
+#define CUHC_ERROR_NON_FINITE (-6)
+/* Additions: a bounded device wait ran out; a size beyond an entry point's limit. */
+#define CUHC_ERROR_TIMEOUT (-7)
+#define CUHC_ERROR_TOO_LARGE (-8)
+
+/* distances (numPointsA x numPointsB, row-major) = metric(A[i], B[j]);
+ * pointsB == NULL means B = A.
+ * Replaces reference capi.cu:138-173 (cuhc_pairwise_distances). */
+int cuhc_pairwise_distances(const float *pointsA, int numPointsA, const float *pointsB,
+                            int numPointsB, int numFeatures, int metricId, float metricParam,
+                            float *distances);
+
+/* Full merge tree in scipy's linkage format: tree receives (numPoints - 1) x 4
+ * doubles {id1, id2, height, size}. mst needs single linkage; rnn and
+ * nn_chain need ward with euclidean; dense builds any linkage.
+ * Replaces reference capi.cu:179-257 (cuhc_linkage). */
+int cuhc_linkage(const float *points, int numPoints, int numFeatures, int metricId,
+                 float metricParam, int linkageId, int algorithmId, double *tree);
+
+/* Ward through RNN rounds with explicit hand-over settings (test hook).
+ * Replaces reference capi.cu:261-279 (cuhc_ward_rnn_with_options). */
+int cuhc_ward_rnn_with_options(const float *points, int numPoints, int numFeatures,
+                               float minProgress, int denseBelow, int allowDense, double *tree);
+
+/* HDBSCAN's single-linkage tree of mutual reachability,
+ * max(core_i, core_j, d(i, j) / alpha); core (may be NULL) receives the core
+ * distances (distance to the minSamples-th nearest point, itself first).
+ * Replaces reference capi.cu:285-309 (cuhc_hdbscan_tree). */
+int cuhc_hdbscan_tree(const float *points, int numPoints, int numFeatures, int metricId,
+                      float metricParam, int minSamples, float alpha, int coreMethod,
+                      double *tree, float *core);
+
+/* HDBSCAN's condensed tree of a (numPoints - 1) x 4 tree: up to capacity rows
+ * into the four arrays; returns the row count, or -(rows needed).
+ * Replaces reference capi.cu:314-327 (cuhc_condense_tree). */
+long long cuhc_condense_tree(const double *tree, long long numPoints, long long minClusterSize,
+                             long long capacity, long long *parent, long long *child,
+                             double *lambda, long long *size);
+
+/* Spatial pruning of the matrix-free paths; results never change.
+ * Replaces reference capi.cu:332-337 (cuhc_set_pruning). */
+int cuhc_set_pruning(int mode);
+
+/* Tiles computed and tiles in total by the passes since the last call; resets.
+ * Replaces reference capi.cu:341-345 (cuhc_prune_stats). */
+void cuhc_prune_stats(unsigned long long *computed, unsigned long long *total);
+
+/* Message for a status code.
+ * Replaces reference capi.cu:347-364 (cuhc_error_string). */
+const char *cuhc_error_string(int code);
+
+/* ---- additions (no counterpart in the reference) ------------------------ */
+
+/* cuhc_linkage with the points already in device memory (current device). */
+int cuhc_linkage_device(const float *devicePoints, int numPoints, int numFeatures, int metricId,
+                        float metricParam, int linkageId, int algorithmId, double *tree);
+
+/* cuhc_hdbscan_tree with the points already in device memory. */
+int cuhc_hdbscan_tree_device(const float *devicePoints, int numPoints, int numFeatures,
+                             int metricId, float metricParam, int minSamples, float alpha,
+                             int coreMethod, double *tree, float *core);
+
+/* Cumulative counters since load: out[0] tiles computed, out[1] tiles in all
+ * passes, out[2] passes, out[3] Borůvka rounds (first `count` of them). */
+int cuhc_pass_stats(unsigned long long *out, int count);
+
+/* Number of this library's own kernel launches since load. */
+unsigned long long cuhc_launch_count(void);
+
+/* Per-pass CUDA-event timing on the launching stream: on != 0 switches it on. */
+int cuhc_set_timing(int on);
+
+/* Per pass kind (0 k-NN pass, 1 nearest-other-component pass, 2 screened
+ * pass): device milliseconds, launches and tiles computed since the last
+ * call (first `count` kinds); resets them. */
+int cuhc_kernel_timing(double *ms, unsigned long long *launches, unsigned long long *tiles,
+                       int count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUHC_B200_CUHC_H */
