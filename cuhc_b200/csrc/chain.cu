@@ -160,7 +160,12 @@ __global__ void __launch_bounds__(kChainThreads) chainKernel(ChainState s) {
         }
         const int nearest = s0 == -1 ? prev : s0;
         redDist[0] = d0;
-        if (nearest == prev) {
+        if (nearest < 0 || nearest >= s.m) {
+          // No comparable candidate (NaN distances): stop with an error.
+          atomicCAS(s.error, 0, (int)kErrorNonFinite);
+          mergeWith = -1;
+          *s.current = -1;
+        } else if (nearest == prev) {
           mergeWith = prev;
         } else {
           mergeWith = -1;

@@ -219,8 +219,10 @@ __global__ void denseMerge(DenseState s) {
   }
 }
 
+// Next step; stays at n - 1 after the last merge, and at n after an early
+// stop (no finite pair left), which the host reports as an error.
 __global__ void denseAdvance(DenseState s) {
-  if (*s.step < s.n)
+  if (*s.step < s.n - 1)
     ++*s.step;
 }
 
