@@ -101,6 +101,20 @@ int cuhc_hdbscan_tree_device(const float *devicePoints, int numPoints, int numFe
  * passes, out[2] passes, out[3] Borůvka rounds (first `count` of them). */
 int cuhc_pass_stats(unsigned long long *out, int count);
 
+/* cuhc_pairwise_distances for callers that cannot allocate GPU memory (a
+ * host framework owns every device allocation, or an allocation on this path
+ * could block or fail). No counterpart in the reference. A, B (NULL means
+ * B = A, then numPointsB == numPointsA) and the output are DEVICE memory; the
+ * kernel's scratch is a fixed 32 MiB device array inside the library, shared
+ * by all calls, so calls that overlap on the GPU race. The work is enqueued
+ * on `stream` (NULL: default stream) and not waited for. The first call on a
+ * device sets up the array's address; make it before any stream capture.
+ * Inputs whose tiled copies exceed the 32 MiB return CUHC_ERROR_TOO_LARGE. */
+int cuhc_pairwise_distances_noalloc(const float *devicePointsA, int numPointsA,
+                                    const float *devicePointsB, int numPointsB, int numFeatures,
+                                    int metricId, float metricParam, float *deviceDistances,
+                                    void *stream);
+
 /* Number of this library's own kernel launches since load. */
 unsigned long long cuhc_launch_count(void);
 
