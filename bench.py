@@ -197,6 +197,8 @@ def main():
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--n", type=int, default=N_POINTS,
+                        help="points of the same recipe (smaller cases for profiling)")
     args = parser.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -221,7 +223,7 @@ def main():
     sys.path.insert(0, HERE)
     from cuhc_b200 import _lib  # noqa: PLC0415
 
-    X = make_blobs_with_noise()
+    X = make_blobs_with_noise(n=args.n)
     n, d = X.shape
     f32, f64 = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)
     X_dev = torch.from_numpy(X).cuda()
@@ -308,7 +310,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 2),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "hdbscan 1,000,000 x 8, 20 blobs + 10% noise, min_samples 25",
+            "config": {"workload": f"hdbscan {n:,} x 8, 20 blobs + 10% noise, min_samples 25",
                        "n": n, "d": d, "min_samples": MIN_SAMPLES, "path": "plain exact fp32",
                        "l2": "flushed before every step (256 MB write)",
                        "parallelism": f"replicas x{world}"},

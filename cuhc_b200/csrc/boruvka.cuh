@@ -165,7 +165,7 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
   DeviceBuffer<int> comp, parent, counters, error;
   DeviceBuffer<unsigned long long> nearest, compKey, tiles;
   DeviceBuffer<unsigned int> compBest, compV;
-  CUHC_TRY(st, comp.allocate(n, stream));
+  CUHC_TRY(st, comp.allocate(paddedToTiles(n), stream));
   CUHC_TRY(st, parent.allocate(n, stream));
   CUHC_TRY(st, counters.allocate(4, stream));
   CUHC_TRY(st, error.allocate(1, stream));

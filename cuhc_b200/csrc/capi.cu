@@ -127,7 +127,7 @@ int hdbscanTree(const float *devPoints, int n, int d, const Metric &m, int minSa
   const bool prune = shouldPrune<Metric>(n, d);
   CUHC_TRY(st, index.build(devPoints, n, d, prune, s));
   DeviceBuffer<float> core, coreOrig;
-  CUHC_TRY(st, core.allocate(n, s));
+  CUHC_TRY(st, core.allocate(paddedToTiles(n), s));
   PassStats stats;
   CUHC_TRY(st, coreDistances<Metric>(index, m, minSamples, prune, core.get(), &stats, s));
   CUHC_TRY(st, index.updateMinValues(core.get()));

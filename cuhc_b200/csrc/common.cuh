@@ -110,6 +110,11 @@ constexpr int kTile = 128;
 
 inline int numTilesFor(int n) { return (n + kTile - 1) / kTile; }
 
+// Entries of a per-position array padded to whole tiles: the passes copy a
+// tile's 128 entries with one bulk copy, which must stay inside the
+// allocation. Padding entries are never used as data.
+inline size_t paddedToTiles(int n) { return (size_t)numTilesFor(n) * kTile; }
+
 // Feature chunk width of the tiled point layout: features are stored per
 // tile in chunks of KC (4/8/16/32), feature-major within a chunk, zero padded.
 inline int chunkWidthFor(int d) { return d <= 4 ? 4 : d <= 8 ? 8 : d <= 16 ? 16 : 32; }

@@ -1,31 +1,73 @@
-// The two all-pairs pass kernels (see engine.cuh for the block shape):
+// The all-pairs pass kernel (see engine.cuh for the block shape), in two
+// modes:
 //
-//   nearestPassKernel  for every point, its minimum-weight edge to a point of
-//                      another component, key (weight bits, original index);
-//                      the Borůvka step (single linkage, HDBSCAN) and the
-//                      RNN-Ward nearest-cluster step (every slot its own
-//                      component). Same result as the reference's
-//                      nearestOtherComponent{,Symmetric,Walk}Kernel
-//                      (distance_matrix.cuh:228-390, spatial.cuh:215-343) for
-//                      every row whose component can still win; rows of a
-//                      component whose best edge is known to be lighter may
-//                      stop early, which never changes the component minimum.
-//   knnPassKernel      for every point, the k-th smallest distance with the
-//                      point itself counted as 0 (HDBSCAN core distances);
-//                      same values as the reference's kthNearestFusedKernel
-//                      (hdbscan.cuh:144-258).
+//   nearest  for every point, its minimum-weight edge to a point of another
+//            component, key (weight bits, original index): the Borůvka step
+//            (single linkage, HDBSCAN) and the RNN-Ward nearest-cluster step
+//            (every slot its own component). Same result as the reference's
+//            nearestOtherComponent{,Symmetric,Walk}Kernel
+//            (distance_matrix.cuh:228-390, spatial.cuh:215-343) for every row
+//            whose component can still win; rows of a component whose best
+//            edge is known to be lighter may stop early, which never changes
+//            the component minimum.
+//   knn      for every point, the k-th smallest distance with the point
+//            itself counted as 0 (HDBSCAN core distances); the values of the
+//            reference's kthNearestFusedKernel (hdbscan.cuh:144-258).
+//
+// Schedule of a block (one row tile):
+//   1. the row tile against itself (seeds every row's threshold);
+//   2. warp 0 collects candidate column tiles: it pops up to 32 BVH nodes at
+//      a time from a shared frontier, one node per lane, tests each node's
+//      weight lower bound against the block threshold, and appends surviving
+//      leaves to a shared candidate list (up to kListCap per batch);
+//   3. the list is sorted by lower bound (bitonic, in shared memory), so the
+//      tiles are visited nearest first and thresholds tighten early;
+//   4. the tiles are computed in that order. While tile i is computed, the
+//      tensor memory accelerator copies tile i+1 (its feature block and its
+//      original-index / component / value rows) into the other half of a
+//      double buffer (cp.async.bulk on an mbarrier); a candidate whose bound
+//      now exceeds the tightened threshold is skipped;
+//   5. repeat from 2 until the frontier is empty.
 #pragma once
 
-#include "profiling.cuh"
+#include "asyncload.cuh"
 #include "engine.cuh"
+#include "profiling.cuh"
 
 namespace cuhc {
 
-// Threads 0..127 (one row each) refresh the row filters and the tile
+constexpr int kListCap = 1024;
+// The frontier is a stack popped 32 at a time, each pop pushing at most two
+// children one level deeper: it holds at most ~64 nodes per tree level, and
+// the tile tree of 2^31 points is 24 levels deep. A full frontier stops the
+// pass with an error (never a hang).
+constexpr int kFrontierCap = 2048;
+
+// Shared state of a pass block besides the staged tiles.
+struct PassState {
+  unsigned long long rowBest[kTile];
+  float rowFilter[kTile];
+  float warpMax[kThreads / 32];
+  int listTile[kListCap];
+  float listLb[kListCap];
+  int frontNode[kFrontierCap];
+  uint64_t bar[2];
+  float thrTile;
+  int listLen, frontLen, overflow;
+};
+
+// Column metadata of a staged tile (bulk-copy destinations, 512 B each).
+struct ColumnMeta {
+  int *orig;
+  int *comp;
+  float *value;
+};
+
+// Threads 0..127 (one row each) refresh the row filters and the block
 // threshold; everyone must call it (it synchronizes).
 template <class Metric, class Weight, bool kKnn>
 __device__ __forceinline__ void refreshThresholds(const PassParams &p, const Metric &m,
-                                                  const Weight &w, PassShared &sh,
+                                                  const Weight &w, PassState &sh,
                                                   const float *lists, int firstRow) {
   const int tid = threadIdx.x;
   float t = -INFINITY;
@@ -68,26 +110,14 @@ __device__ __forceinline__ void refreshThresholds(const PassParams &p, const Met
   __syncthreads();
 }
 
-// Column data of tile J into shared memory (threads 0..127).
-template <class Weight>
-__device__ __forceinline__ void loadColumns(const PassParams &p, const Weight &w, PassShared &sh,
-                                            int tileJ) {
-  const int tid = threadIdx.x;
-  if (tid < kTile) {
-    const int pos = tileJ * kTile + tid;
-    const bool valid = pos < p.n;
-    const int orig = valid ? p.order[pos] : -1;
-    sh.colOrig[tid] = orig;
-    sh.colComp[tid] = valid ? (p.component ? p.component[pos] : orig) : -1;
-    sh.colValue[tid] = valid ? w.load(pos) : 0.0f;
-  }
-}
-
-template <class Metric, class Weight, int KC>
-__device__ __forceinline__ void nearestEpilogue(const Metric &m, const Weight &w, PassShared &sh,
+template <class Metric, class Weight>
+__device__ __forceinline__ void nearestEpilogue(const Metric &m, const Weight &w,
+                                                const PassState &sh, const ColumnMeta &cm,
                                                 typename Metric::Acc (&acc)[8][8],
                                                 const int (&rowComp)[8],
-                                                const float (&rowVal)[8], const TileGeom &g) {
+                                                const float (&rowVal)[8], int firstCol, int n,
+                                                bool useComp, bool useValue, const TileGeom &g,
+                                                unsigned long long *rowBest) {
   float F[8];
   int cComp[8], cOrig[8];
   float cVal[8];
@@ -97,9 +127,10 @@ __device__ __forceinline__ void nearestEpilogue(const Metric &m, const Weight &w
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
     const int col = g.col(c);
-    cComp[c] = sh.colComp[col];
-    cOrig[c] = sh.colOrig[col];
-    cVal[c] = sh.colValue[col];
+    const bool valid = firstCol + col < n;
+    cOrig[c] = valid ? cm.orig[col] : -1;
+    cComp[c] = valid ? (useComp ? cm.comp[col] : cOrig[c]) : -1;
+    cVal[c] = useValue ? cm.value[col] : 0.0f;
   }
   bool any = false;
 #pragma unroll
@@ -135,8 +166,8 @@ __device__ __forceinline__ void nearestEpilogue(const Metric &m, const Weight &w
       const unsigned long long other = __shfl_xor_sync(0xffffffffu, best, off);
       best = other < best ? other : best;
     }
-    if (g.tc == 0 && best < sh.rowBest[g.row(r)])
-      sh.rowBest[g.row(r)] = best;
+    if (g.tc == 0 && best < rowBest[g.row(r)])
+      rowBest[g.row(r)] = best;
   }
 }
 
@@ -152,9 +183,10 @@ __device__ __forceinline__ void insertSorted(float *list, int k, float v) {
 }
 
 template <class Metric>
-__device__ __forceinline__ void knnEpilogue(const Metric &m, PassShared &sh, float *lists, int k,
-                                            typename Metric::Acc (&acc)[8][8], int firstRow,
-                                            int firstCol, int n, const TileGeom &g) {
+__device__ __forceinline__ void knnEpilogue(const Metric &m, const PassState &sh, float *lists,
+                                            int k, typename Metric::Acc (&acc)[8][8],
+                                            int firstRow, int firstCol, int n,
+                                            const TileGeom &g) {
   const int lane = threadIdx.x & 31;
   const unsigned groupMask = (lane < 16) ? 0x0000ffffu : 0xffff0000u;
 #pragma unroll
@@ -167,7 +199,7 @@ __device__ __forceinline__ void knnEpilogue(const Metric &m, PassShared &sh, flo
     if (rowPos < n) {
 #pragma unroll
       for (int c = 0; c < 8; ++c)
-        if (sh.colOrig[g.col(c)] >= 0 && m.filter(acc[r][c]) <= F)
+        if (firstCol + g.col(c) < n && m.filter(acc[r][c]) <= F)
           pending |= 1u << c;
     }
     while (true) {
@@ -193,16 +225,127 @@ __device__ __forceinline__ void knnEpilogue(const Metric &m, PassShared &sh, flo
   }
 }
 
+// Warp 0: collects candidate column tiles into sh.listTile / listLb, until the
+// frontier is empty or the list is nearly full. Nodes whose bound exceeds the
+// block threshold are dropped; subtrees of the row tile's own single
+// component are skipped.
+template <class Metric, class Weight>
+__device__ void collectCandidates(const PassParams &p, const Metric &m, const Weight &w,
+                                  PassState &sh, const float *rowLow, const float *rowHigh,
+                                  int rowTile, int rowPure, float rowMinValue, float slack) {
+  const int lane = threadIdx.x & 31;
+  const float thr = sh.thrTile;
+  int listLen = 0;
+  int frontLen = sh.frontLen;
+  while (frontLen > 0 && listLen <= kListCap - 32) {
+    const int take = min(32, min(frontLen, kFrontierCap - frontLen));
+    if (take == 0) {
+      if (lane == 0)
+        sh.overflow = 1;
+      break;
+    }
+    int node = -1;
+    if (lane < take)
+      node = sh.frontNode[frontLen - 1 - lane];
+    __syncwarp();
+    frontLen -= take;
+    bool keepLeaf = false, expand = false;
+    int tile = -1;
+    float lb = 0.0f;
+    if (node >= 0) {
+      const int pure = p.nodePure ? p.nodePure[node] : -1;
+      const bool skip = rowPure >= 0 && pure == rowPure;
+      if (!skip && p.prune && Metric::kBoxBound) {
+        typename Metric::Acc acc = m.init();
+        const float *lo = p.nodeLow + (size_t)node * p.d, *hi = p.nodeHigh + (size_t)node * p.d;
+        for (int f = 0; f < p.d; ++f) {
+          const float gap =
+              fmaxf(0.0f, fmaxf(__ldg(lo + f) - rowHigh[f], rowLow[f] - __ldg(hi + f)));
+          acc = m.accumulate(acc, gap, 0.0f);
+        }
+        const float v = p.nodeMinValue ? p.nodeMinValue[node] : 0.0f;
+        lb = w.lowerBound(m.finalize(acc), rowMinValue, v) * slack;
+      }
+      if (!skip && lb <= thr) {
+        if (p.nodeLeft[node] < 0) {
+          tile = p.nodeFirstTile[node];
+          keepLeaf = tile != rowTile;
+        } else {
+          expand = true;
+        }
+      }
+    }
+    const unsigned leaves = __ballot_sync(0xffffffffu, keepLeaf);
+    const unsigned inner = __ballot_sync(0xffffffffu, expand);
+    const unsigned below = (1u << lane) - 1;
+    if (keepLeaf) {
+      const int at = listLen + __popc(leaves & below);
+      sh.listTile[at] = tile;
+      sh.listLb[at] = lb;
+    }
+    if (expand) {
+      const int at = frontLen + 2 * __popc(inner & below);
+      sh.frontNode[at] = p.nodeLeft[node];
+      sh.frontNode[at + 1] = p.nodeRight[node];
+    }
+    listLen += __popc(leaves);
+    frontLen += 2 * __popc(inner);
+    __syncwarp();
+  }
+  if (lane == 0) {
+    sh.listLen = listLen;
+    sh.frontLen = frontLen;
+  }
+}
+
+// Sorts the first `len` candidates by lower bound (bitonic network over the
+// next power of two, padding with +inf). All threads call it.
+__device__ __forceinline__ void sortCandidates(PassState &sh, int len) {
+  int size = 1;
+  while (size < len)
+    size *= 2;
+  for (int i = len + threadIdx.x; i < size; i += kThreads) {
+    sh.listLb[i] = INFINITY;
+    sh.listTile[i] = -1;
+  }
+  __syncthreads();
+  for (int k = 2; k <= size; k *= 2) {
+    for (int j = k / 2; j > 0; j /= 2) {
+      for (int i = threadIdx.x; i < size / 2; i += kThreads) {
+        const int lo = 2 * j * (i / j) + (i % j), hi = lo + j;
+        const bool ascending = (lo & k) == 0;
+        const float a = sh.listLb[lo], b = sh.listLb[hi];
+        if ((a > b) == ascending) {
+          sh.listLb[lo] = b;
+          sh.listLb[hi] = a;
+          const int t = sh.listTile[lo];
+          sh.listTile[lo] = sh.listTile[hi];
+          sh.listTile[hi] = t;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
 template <class Metric, class Weight, int KC, bool kKnn>
-__global__ void __launch_bounds__(kThreads, 2)
-    passKernel(PassParams p, Metric m, Weight w) {
-  extern __shared__ __align__(16) float dyn[];
-  __shared__ PassShared sh;
+__global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m, Weight w) {
+  extern __shared__ __align__(128) float dyn[];
+  __shared__ PassState sh;
+  // Dynamic layout: row tile, two column-tile buffers, two metadata buffers,
+  // row box, k-NN lists. Every bulk-copy destination is 512-byte aligned.
   float *sA = dyn;
-  float *sB = sA + KC * kTile;
-  float *rowLow = sB + KC * kTile;
+  float *sB[2] = {sA + KC * kTile, sA + 2 * KC * kTile};
+  int *metaBase = (int *)(sA + 3 * KC * kTile);
+  ColumnMeta meta[2];
+  for (int b = 0; b < 2; ++b) {
+    meta[b].orig = metaBase + b * 3 * kTile;
+    meta[b].comp = metaBase + b * 3 * kTile + kTile;
+    meta[b].value = (float *)(metaBase + b * 3 * kTile + 2 * kTile);
+  }
+  float *rowLow = (float *)(metaBase + 6 * kTile);
   float *rowHigh = rowLow + p.d;
-  float *lists = rowHigh + p.d; // knn only: [128][k]
+  float *lists = rowHigh + p.d;
 
   const TileGeom g;
   const int tid = threadIdx.x;
@@ -212,6 +355,9 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int rowPure = (!kKnn && p.nodePure) ? p.nodePure[leaf] : -1;
   const float rowMinValue = p.nodeMinValue ? p.nodeMinValue[leaf] : 0.0f;
   const float slack = 1.0f - boxSlack(p.d);
+  const bool useComp = !kKnn && p.component != nullptr;
+  const bool useValue = !kKnn && w.value != nullptr;
+  const size_t tileFloats = (size_t)p.numChunks * KC * kTile;
 
   int rowComp[8];
   float rowVal[8];
@@ -232,47 +378,168 @@ __global__ void __launch_bounds__(kThreads, 2)
     rowHigh[f] = p.nodeHigh[(size_t)leaf * p.d + f];
   }
   if (p.numChunks == 1)
-    copyChunk(sA, p.tiled + (size_t)I * KC * kTile, KC * kTile);
+    copyChunk(sA, p.tiled + (size_t)I * tileFloats, KC * kTile);
   if (tid == 0) {
-    sh.sp = 0;
+    mbarrierInit(&sh.bar[0], 1);
+    mbarrierInit(&sh.bar[1], 1);
+    fenceBarrierInit();
+    sh.frontLen = 0;
     sh.overflow = 0;
-    const int root = 0;
-    const int rootPure = p.nodePure && !kKnn ? p.nodePure[root] : -1;
+    const int rootPure = (!kKnn && p.nodePure) ? p.nodePure[0] : -1;
     if (!(rowPure >= 0 && rootPure == rowPure)) {
-      sh.stackNode[0] = root;
-      sh.stackLb[0] = 0.0f;
-      sh.sp = 1;
+      sh.frontNode[0] = 0;
+      sh.frontLen = 1;
     }
+  }
+  // Column metadata of the row tile itself, for the self tile.
+  if (tid < kTile) {
+    const int pos = firstRow + tid;
+    const bool valid = pos < p.n;
+    meta[0].orig[tid] = valid ? p.order[pos] : -1;
+    if (useComp)
+      meta[0].comp[tid] = valid ? p.component[pos] : -1;
+    if (useValue)
+      meta[0].value[tid] = valid ? w.load(pos) : 0.0f;
   }
   __syncthreads();
   refreshThresholds<Metric, Weight, kKnn>(p, m, w, sh, lists, firstRow);
 
   unsigned long long computed = 0;
-  // The row tile against itself first: it seeds every threshold with the
-  // nearest points in space. A tile whose points share one component has no
-  // edge inside.
-  int J = rowPure >= 0 ? -1 : I;
-  while (true) {
-    if (J >= 0) {
-      loadColumns(p, w, sh, J);
-      typename Metric::Acc acc[8][8];
-      computeTile<Metric, KC>(p.tiled, p.tiled, p.numChunks, I, J, sA, sB, m, acc, g);
-      if (kKnn)
-        knnEpilogue(m, sh, lists, p.k, acc, firstRow, J * kTile, p.n, g);
-      else
-        nearestEpilogue<Metric, Weight, KC>(m, w, sh, acc, rowComp, rowVal, g);
-      __syncthreads();
-      refreshThresholds<Metric, Weight, kKnn>(p, m, w, sh, lists, firstRow);
-      ++computed;
-    }
-    if (tid < 32)
-      traverseNext(p, m, w, sh, rowLow, rowHigh, I, rowPure, rowMinValue, slack);
+  bool failed = false;
+
+  // Accumulate + epilogue of one staged column tile.
+  auto processTile = [&](int J, const float *bTile, const ColumnMeta &cm) {
+    typename Metric::Acc acc[8][8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        acc[r][c] = m.init();
+    accumulateChunk<Metric, KC>(sA, bTile, m, acc, g);
+    if (kKnn)
+      knnEpilogue(m, sh, lists, p.k, acc, firstRow, J * kTile, p.n, g);
+    else
+      nearestEpilogue<Metric, Weight>(m, w, sh, cm, acc, rowComp, rowVal, J * kTile, p.n,
+                                      useComp, useValue, g, sh.rowBest);
     __syncthreads();
-    J = sh.next;
-    if (J < 0)
+    refreshThresholds<Metric, Weight, kKnn>(p, m, w, sh, lists, firstRow);
+    ++computed;
+  };
+  // The general path (features in several chunks): synchronous staging.
+  auto processTileChunked = [&](int J) {
+    if (tid < kTile) {
+      const int pos = J * kTile + tid;
+      const bool valid = pos < p.n;
+      meta[0].orig[tid] = valid ? p.order[pos] : -1;
+      if (useComp)
+        meta[0].comp[tid] = valid ? p.component[pos] : -1;
+      if (useValue)
+        meta[0].value[tid] = valid ? w.load(pos) : 0.0f;
+    }
+    typename Metric::Acc acc[8][8];
+    computeTile<Metric, KC>(p.tiled, p.tiled, p.numChunks, I, J, sA, sB[0], m, acc, g);
+    if (kKnn)
+      knnEpilogue(m, sh, lists, p.k, acc, firstRow, J * kTile, p.n, g);
+    else
+      nearestEpilogue<Metric, Weight>(m, w, sh, meta[0], acc, rowComp, rowVal, J * kTile, p.n,
+                                      useComp, useValue, g, sh.rowBest);
+    __syncthreads();
+    refreshThresholds<Metric, Weight, kKnn>(p, m, w, sh, lists, firstRow);
+    ++computed;
+  };
+
+  // 1. The row tile against itself (none if all its points share one
+  //    component: no edge inside).
+  if (rowPure < 0) {
+    if (p.numChunks == 1)
+      processTile(I, sA, meta[0]);
+    else
+      processTileChunked(I);
+  }
+
+  // Issues the bulk copies of candidate `i` into buffer b (thread 0).
+  const uint32_t metaBytes = (uint32_t)(kTile * sizeof(int)) * (1 + useComp + useValue);
+  const uint32_t tileBytes = (uint32_t)(KC * kTile * sizeof(float));
+  auto issue = [&](int i, int b) {
+    const int J = sh.listTile[i];
+    fenceProxyAsync();
+    mbarrierArriveExpectTx(&sh.bar[b], tileBytes + metaBytes);
+    bulkCopyToShared(sB[b], p.tiled + (size_t)J * tileFloats, tileBytes, &sh.bar[b]);
+    bulkCopyToShared(meta[b].orig, p.order + (size_t)J * kTile, kTile * sizeof(int), &sh.bar[b]);
+    if (useComp)
+      bulkCopyToShared(meta[b].comp, p.component + (size_t)J * kTile, kTile * sizeof(int),
+                       &sh.bar[b]);
+    if (useValue)
+      bulkCopyToShared(meta[b].value, w.value + (size_t)J * kTile, kTile * sizeof(float),
+                       &sh.bar[b]);
+  };
+  uint32_t phase[2] = {0, 0};
+  bool inFlight[2] = {false, false};
+
+  while (!failed) {
+    // 2. Candidates of this batch.
+    if (tid < 32)
+      collectCandidates(p, m, w, sh, rowLow, rowHigh, I, rowPure, rowMinValue, slack);
+    __syncthreads();
+    const int len = sh.listLen;
+    if (sh.overflow) {
+      failed = true;
+      break;
+    }
+    if (len == 0 && sh.frontLen == 0)
+      break;
+    // 3. Nearest first.
+    if (p.prune && Metric::kBoxBound && len > 1)
+      sortCandidates(sh, len);
+    // 4. Compute them.
+    if (p.numChunks == 1) {
+      auto nextValid = [&](int from) {
+        while (from < len && sh.listLb[from] > sh.thrTile)
+          ++from;
+        return from;
+      };
+      int cur = nextValid(0), buf = 0;
+      if (cur < len) {
+        if (tid == 0)
+          issue(cur, buf);
+        inFlight[buf] = true;
+      }
+      while (cur < len) {
+        const int next = nextValid(cur + 1);
+        if (next < len) {
+          if (tid == 0)
+            issue(next, buf ^ 1);
+          inFlight[buf ^ 1] = true;
+        }
+        const bool ready = mbarrierWait(&sh.bar[buf], phase[buf]);
+        phase[buf] ^= 1;
+        inFlight[buf] = false;
+        if (__syncthreads_or(!ready)) {
+          failed = true;
+          break;
+        }
+        if (sh.listLb[cur] <= sh.thrTile)
+          processTile(sh.listTile[cur], sB[buf], meta[buf]);
+        else
+          __syncthreads(); // nobody reads this buffer any more
+        cur = next;
+        buf ^= 1;
+      }
+    } else {
+      for (int i = 0; i < len; ++i)
+        if (sh.listLb[i] <= sh.thrTile)
+          processTileChunked(sh.listTile[i]);
+    }
+    __syncthreads();
+    if (sh.frontLen == 0)
       break;
   }
 
+  // After a failed wait, give copies still in flight a bounded chance to land
+  // before the block's shared memory is released.
+  for (int b = 0; b < 2; ++b)
+    if (inFlight[b])
+      mbarrierWait(&sh.bar[b], phase[b]);
   if (tid < kTile) {
     const int pos = firstRow + tid;
     if (pos < p.n) {
@@ -285,8 +552,8 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (tid == 0) {
     if (p.tilesComputed)
       atomicAdd(p.tilesComputed, computed);
-    if (sh.overflow && p.error)
-      atomicCAS(p.error, 0, (int)kErrorTooLarge);
+    if (failed && p.error)
+      atomicCAS(p.error, 0, sh.overflow ? (int)kErrorTooLarge : (int)kErrorTimeout);
   }
 }
 
@@ -294,16 +561,22 @@ __global__ void __launch_bounds__(kThreads, 2)
 template <class Metric, class Weight, bool kKnn>
 int launchPass(const PassParams &p, const Metric &m, const Weight &w, int kc,
                cudaStream_t stream) {
-  const size_t dynBytes =
-      (size_t)(2 * kc * kTile + 2 * p.d + (kKnn ? kTile * p.k : 0)) * sizeof(float);
+  const size_t dynBytes = (size_t)3 * kc * kTile * sizeof(float) + 6 * kTile * sizeof(int) +
+                          (size_t)(2 * p.d + (kKnn ? kTile * p.k : 0)) * sizeof(float);
+  // Bulk copies need 16-byte aligned sources (pool allocations are 256-byte
+  // aligned; refuse anything else rather than fault).
+  auto misaligned = [](const void *ptr) { return ((uintptr_t)ptr & 15) != 0; };
+  if (misaligned(p.tiled) || misaligned(p.order) || misaligned(p.component) ||
+      misaligned(w.value))
+    return (int)cudaErrorMisalignedAddress;
   auto run = [&](auto kernel) {
-    if (dynBytes > 48 * 1024) {
-      const cudaError_t e =
-          cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dynBytes);
-      if (e != cudaSuccess)
-        return (int)e;
-    }
-    kernel<<<p.numTiles, kThreads, dynBytes, stream>>>(p, m, w); noteLaunch();
+    // Static (~18 KB) plus dynamic shared memory can pass the 48 KB default.
+    const cudaError_t e =
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dynBytes);
+    if (e != cudaSuccess)
+      return (int)e;
+    kernel<<<p.numTiles, kThreads, dynBytes, stream>>>(p, m, w);
+    noteLaunch();
     return (int)cudaGetLastError();
   };
   switch (kc) {

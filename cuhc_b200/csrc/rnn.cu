@@ -214,9 +214,9 @@ int rnnWard(const float *devPoints, int n, int d, const RnnOptions &options, dou
   DeviceBuffer<unsigned long long> nearest, tiles;
   for (int b = 0; b < 2; ++b) {
     CUHC_TRY(st, cent[b].allocate((size_t)n * d, s));
-    CUHC_TRY(st, sizeF[b].allocate(n, s));
+    CUHC_TRY(st, sizeF[b].allocate(paddedToTiles(n), s));
     CUHC_TRY(st, size[b].allocate(n, s));
-    CUHC_TRY(st, rep[b].allocate(n, s));
+    CUHC_TRY(st, rep[b].allocate(paddedToTiles(n), s));
   }
   CUHC_TRY(st, slotOfRep.allocate(n, s));
   CUHC_TRY(st, partner.allocate(n, s));

@@ -266,7 +266,7 @@ int SpatialIndex::build(const float *points, int n_, int d_, bool spatial, cudaS
   topo.build(numTiles);
   StatusChain st;
   const int N = topo.numNodes;
-  CUHC_TRY(st, order.allocate(n, s));
+  CUHC_TRY(st, order.allocate(paddedToTiles(n), s));
   CUHC_TRY(st, rank.allocate(n, s));
   CUHC_TRY(st, nodeLeft.allocate(N, s));
   CUHC_TRY(st, nodeRight.allocate(N, s));
