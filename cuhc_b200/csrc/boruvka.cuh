@@ -215,6 +215,7 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
       noteLaunch();
     }
     CUHC_TRY(st, cudaGetLastError());
+    p.singletons = rounds == 0;
     {
       PassTimer timer(kTimerNearestPass, stream);
       CUHC_TRY(st, (launchPass<Metric, Weight, false>(p, metric, weight, index.kc, stream)));

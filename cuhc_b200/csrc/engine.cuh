@@ -62,11 +62,27 @@ __device__ __forceinline__ void accumulateChunk(const float *__restrict__ sA,
     const float4 b1 = reinterpret_cast<const float4 *>(sB + k * kTile + 64)[g.tc];
     const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
     const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+    if constexpr (Metric::kPacked) {
+      // Two adjacent columns per packed instruction.
+      const float2 b2[4] = {make_float2(b[0], b[1]), make_float2(b[2], b[3]),
+                            make_float2(b[4], b[5]), make_float2(b[6], b[7])};
 #pragma unroll
-    for (int r = 0; r < 8; ++r)
+      for (int r = 0; r < 8; ++r) {
+        const float2 negA = make_float2(-a[r], -a[r]);
 #pragma unroll
-      for (int c = 0; c < 8; ++c)
-        acc[r][c] = m.accumulate(acc[r][c], a[r], b[c]);
+        for (int c = 0; c < 4; ++c) {
+          const float2 s = m.accumulate2(make_float2(acc[r][2 * c], acc[r][2 * c + 1]), negA, b2[c]);
+          acc[r][2 * c] = s.x;
+          acc[r][2 * c + 1] = s.y;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+          acc[r][c] = m.accumulate(acc[r][c], a[r], b[c]);
+    }
   }
 }
 
@@ -133,6 +149,7 @@ struct PassParams {
   const int *nodeLeft, *nodeRight, *nodeFirstTile, *leafOfTile, *nodePure;
   const float *nodeLow, *nodeHigh, *nodeMinValue;
   bool prune;
+  bool singletons;                // every point its own component (first round)
   unsigned long long *nearest;    // nearest-mode output, by position
   unsigned int *compBest;         // float bits by component label (null: none)
   float *core;                    // knn-mode output, by position

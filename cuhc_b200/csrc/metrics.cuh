@@ -43,10 +43,18 @@ struct SqEuclideanMetric {
   using Acc = float;
   static constexpr bool kBoxBound = true;
   static constexpr bool kHasFilter = true;
+  // Two columns per instruction (Blackwell's packed FP32): each lane is the
+  // same IEEE subtraction and fused multiply-add as accumulate(), and
+  // (b - a)^2 == (a - b)^2 exactly, so the bits are those of the scalar fold.
+  static constexpr bool kPacked = true;
   CUHC_HD Acc init() const { return 0.0f; }
   CUHC_HD Acc accumulate(Acc acc, float a, float b) const {
     const float diff = a - b;
     return fmaf(diff, diff, acc);
+  }
+  __device__ __forceinline__ float2 accumulate2(float2 acc, float2 negA, float2 b) const {
+    const float2 diff = __fadd2_rn(b, negA);
+    return __ffma2_rn(diff, diff, acc);
   }
   CUHC_HD Acc combine(Acc x, Acc y) const { return x + y; }
   CUHC_HD float finalize(Acc acc) const { return acc; }
@@ -63,6 +71,7 @@ struct ManhattanMetric {
   using Acc = float;
   static constexpr bool kBoxBound = true;
   static constexpr bool kHasFilter = true;
+  static constexpr bool kPacked = false;
   CUHC_HD Acc init() const { return 0.0f; }
   CUHC_HD Acc accumulate(Acc acc, float a, float b) const { return acc + fabsf(a - b); }
   CUHC_HD Acc combine(Acc x, Acc y) const { return x + y; }
@@ -75,6 +84,7 @@ struct ChebyshevMetric {
   using Acc = float;
   static constexpr bool kBoxBound = true;
   static constexpr bool kHasFilter = true;
+  static constexpr bool kPacked = false;
   CUHC_HD Acc init() const { return 0.0f; }
   CUHC_HD Acc accumulate(Acc acc, float a, float b) const { return fmaxf(acc, fabsf(a - b)); }
   CUHC_HD Acc combine(Acc x, Acc y) const { return fmaxf(x, y); }
@@ -90,6 +100,7 @@ struct MinkowskiMetric {
   using Acc = float;
   static constexpr bool kBoxBound = true;
   static constexpr bool kHasFilter = true;
+  static constexpr bool kPacked = false;
   CUHC_HD Acc init() const { return 0.0f; }
   CUHC_HD Acc accumulate(Acc acc, float a, float b) const {
     const float x = fabsf(a - b);
@@ -112,6 +123,7 @@ struct CosineMetric {
   using Acc = float3;
   static constexpr bool kBoxBound = false;
   static constexpr bool kHasFilter = false;
+  static constexpr bool kPacked = false;
   CUHC_HD Acc init() const { return make_float3(0.0f, 0.0f, 0.0f); }
   CUHC_HD Acc accumulate(Acc acc, float a, float b) const {
     acc.x = fmaf(a, b, acc.x);

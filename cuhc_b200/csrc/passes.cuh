@@ -37,6 +37,8 @@
 namespace cuhc {
 
 constexpr int kListCap = 1024;
+// Flag on a candidate's tile index: all its points share one component.
+constexpr int kPureColumnTile = 1 << 30;
 // The frontier is a stack popped 32 at a time, each pop pushing at most two
 // children one level deeper: it holds at most ~64 nodes per tree level, and
 // the tile tree of 2^31 points is 24 levels deep. A full frontier stops the
@@ -116,8 +118,8 @@ __device__ __forceinline__ void nearestEpilogue(const Metric &m, const Weight &w
                                                 typename Metric::Acc (&acc)[8][8],
                                                 const int (&rowComp)[8],
                                                 const float (&rowVal)[8], int firstCol, int n,
-                                                bool useComp, bool useValue, const TileGeom &g,
-                                                unsigned long long *rowBest) {
+                                                bool useComp, bool useValue, bool mask,
+                                                const TileGeom &g, unsigned long long *rowBest) {
   float F[8];
   int cComp[8], cOrig[8];
   float cVal[8];
@@ -132,18 +134,24 @@ __device__ __forceinline__ void nearestEpilogue(const Metric &m, const Weight &w
     cComp[c] = valid ? (useComp ? cm.comp[col] : cOrig[c]) : -1;
     cVal[c] = useValue ? cm.value[col] : 0.0f;
   }
+  // Fast path: does any pair of the warp pass its row's filter? Without
+  // `mask` the minimum runs over every column, a superset of the pairs that
+  // count, so it can only send more warps to the exact path below; `mask`
+  // (tiles that may hold same-component pairs) excludes them up front.
   bool any = false;
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
     float mn = INFINITY;
-    bool seen = false;
+    if (mask) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      const bool ok = cOrig[c] >= 0 && cComp[c] != rowComp[r];
-      mn = fminf(mn, ok ? m.filter(acc[r][c]) : INFINITY);
-      seen |= ok;
+      for (int c = 0; c < 8; ++c)
+        mn = fminf(mn, cComp[c] != rowComp[r] ? m.filter(acc[r][c]) : INFINITY);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        mn = fminf(mn, m.filter(acc[r][c]));
     }
-    any |= seen && mn <= F[r];
+    any |= mn <= F[r];
   }
   if (!__any_sync(0xffffffffu, any))
     return;
@@ -195,6 +203,12 @@ __device__ __forceinline__ void knnEpilogue(const Metric &m, const PassState &sh
     const int rowPos = firstRow + rowInTile;
     float *list = lists + rowInTile * k;
     const float F = sh.rowFilter[rowInTile];
+    float mn = INFINITY;
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+      mn = fminf(mn, m.filter(acc[r][c]));
+    if (!__any_sync(0xffffffffu, rowPos < n && mn <= F))
+      continue; // no pair of this row group can enter a list
     unsigned pending = 0;
     if (rowPos < n) {
 #pragma unroll
@@ -270,6 +284,8 @@ __device__ void collectCandidates(const PassParams &p, const Metric &m, const We
         if (p.nodeLeft[node] < 0) {
           tile = p.nodeFirstTile[node];
           keepLeaf = tile != rowTile;
+          if (pure >= 0)
+            tile |= kPureColumnTile;
         } else {
           expand = true;
         }
@@ -408,7 +424,11 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
   bool failed = false;
 
   // Accumulate + epilogue of one staged column tile.
-  auto processTile = [&](int J, const float *bTile, const ColumnMeta &cm) {
+  // Masking is needed only where same-component pairs can occur: not in
+  // passes where every point is its own component, not between two tiles
+  // that each hold a single (different) component.
+  const bool maskPass = useComp && !p.singletons;
+  auto processTile = [&](int J, const float *bTile, const ColumnMeta &cm, bool colPure) {
     typename Metric::Acc acc[8][8];
 #pragma unroll
     for (int r = 0; r < 8; ++r)
@@ -420,7 +440,8 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
       knnEpilogue(m, sh, lists, p.k, acc, firstRow, J * kTile, p.n, g);
     else
       nearestEpilogue<Metric, Weight>(m, w, sh, cm, acc, rowComp, rowVal, J * kTile, p.n,
-                                      useComp, useValue, g, sh.rowBest);
+                                      useComp, useValue,
+                                      maskPass && !(rowPure >= 0 && colPure), g, sh.rowBest);
     __syncthreads();
     refreshThresholds<Metric, Weight, kKnn>(p, m, w, sh, lists, firstRow);
     ++computed;
@@ -442,7 +463,7 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
       knnEpilogue(m, sh, lists, p.k, acc, firstRow, J * kTile, p.n, g);
     else
       nearestEpilogue<Metric, Weight>(m, w, sh, meta[0], acc, rowComp, rowVal, J * kTile, p.n,
-                                      useComp, useValue, g, sh.rowBest);
+                                      useComp, useValue, maskPass, g, sh.rowBest);
     __syncthreads();
     refreshThresholds<Metric, Weight, kKnn>(p, m, w, sh, lists, firstRow);
     ++computed;
@@ -452,7 +473,7 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
   //    component: no edge inside).
   if (rowPure < 0) {
     if (p.numChunks == 1)
-      processTile(I, sA, meta[0]);
+      processTile(I, sA, meta[0], false);
     else
       processTileChunked(I);
   }
@@ -461,7 +482,7 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
   const uint32_t metaBytes = (uint32_t)(kTile * sizeof(int)) * (1 + useComp + useValue);
   const uint32_t tileBytes = (uint32_t)(KC * kTile * sizeof(float));
   auto issue = [&](int i, int b) {
-    const int J = sh.listTile[i];
+    const int J = sh.listTile[i] & ~kPureColumnTile;
     fenceProxyAsync();
     mbarrierArriveExpectTx(&sh.bar[b], tileBytes + metaBytes);
     bulkCopyToShared(sB[b], p.tiled + (size_t)J * tileFloats, tileBytes, &sh.bar[b]);
@@ -519,7 +540,8 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
           break;
         }
         if (sh.listLb[cur] <= sh.thrTile)
-          processTile(sh.listTile[cur], sB[buf], meta[buf]);
+          processTile(sh.listTile[cur] & ~kPureColumnTile, sB[buf], meta[buf],
+                      (sh.listTile[cur] & kPureColumnTile) != 0);
         else
           __syncthreads(); // nobody reads this buffer any more
         cur = next;
@@ -528,7 +550,7 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
     } else {
       for (int i = 0; i < len; ++i)
         if (sh.listLb[i] <= sh.thrTile)
-          processTileChunked(sh.listTile[i]);
+          processTileChunked(sh.listTile[i] & ~kPureColumnTile);
     }
     __syncthreads();
     if (sh.frontLen == 0)
