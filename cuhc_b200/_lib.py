@@ -54,6 +54,8 @@ lib.cuhc_pass_stats.argtypes = [_u64, _int]
 lib.cuhc_hdbscan_labels.restype = _int
 lib.cuhc_hdbscan_labels.argtypes = [_f64, ctypes.c_int64, ctypes.c_int64, _int, _int,
                                     ctypes.c_double, ctypes.c_int64, _i64, _f64]
+lib.cuhc_set_screen.restype = _int
+lib.cuhc_set_screen.argtypes = [_int]
 lib.cuhc_launch_count.restype = ctypes.c_uint64
 lib.cuhc_launch_count.argtypes = []
 lib.cuhc_set_timing.restype = _int
@@ -62,8 +64,9 @@ lib.cuhc_kernel_timing.restype = _int
 lib.cuhc_kernel_timing.argtypes = [_f64, _u64, _u64, _int]
 
 PRUNE_MODES = {"auto": 0, "always": 1, "never": 2}
+SCREEN_MODES = {"auto": 0, "on": 1, "off": 2}
 # Pass kinds of cuhc_kernel_timing.
-TIMER_KINDS = ("knn_pass", "nearest_pass", "screen_pass", "reserved")
+TIMER_KINDS = ("knn_pass", "nearest_pass", "screen_pass", "screen_knn_pass")
 # cudaErrorMemoryAllocation, reported by the dense path as MemoryError.
 CUDA_ERROR_OUT_OF_MEMORY = 2
 
@@ -90,6 +93,13 @@ def set_pruning(mode):
     """Spatial pruning of the matrix-free paths: "auto", "always" or "never".
     Results are identical in every mode; only the time changes."""
     check(lib.cuhc_set_pruning(PRUNE_MODES[mode]))
+
+
+def set_screen(mode):
+    """Tensor-core screening of the all-pairs passes: "auto" (on for euclidean
+    and sqeuclidean up to 32 features), "on" or "off". Results are identical
+    in every mode; only the time changes."""
+    check(lib.cuhc_set_screen(SCREEN_MODES[mode]))
 
 
 def prune_stats():

@@ -25,6 +25,7 @@
 #include "profiling.cuh"
 #include "mst.cuh"
 #include "passes.cuh"
+#include "screen.cuh"
 
 namespace cuhc {
 namespace boruvka_detail {
@@ -217,8 +218,12 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
     CUHC_TRY(st, cudaGetLastError());
     p.singletons = rounds == 0;
     {
-      PassTimer timer(kTimerNearestPass, stream);
-      CUHC_TRY(st, (launchPass<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
+      const bool screened = useScreen<Metric>(index.d, 0);
+      PassTimer timer(screened ? kTimerScreenPass : kTimerNearestPass, stream);
+      if (screened)
+        CUHC_TRY(st, (launchScreen<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
+      else
+        CUHC_TRY(st, (launchPass<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
       if (timer.start) {
         unsigned long long tilesNow = 0;
         cudaMemcpyAsync(&tilesNow, tiles.get(), sizeof(tilesNow), cudaMemcpyDeviceToHost, stream);
@@ -321,9 +326,14 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
   p.tilesComputed = tiles.get();
   p.error = error.get();
   {
-    PassTimer timer(kTimerKnnPass, stream);
-    CUHC_TRY(st,
-             (launchPass<Metric, PlainWeight, true>(p, metric, PlainWeight{}, index.kc, stream)));
+    const bool screened = useScreen<Metric>(index.d, k);
+    PassTimer timer(screened ? kTimerScreenKnnPass : kTimerKnnPass, stream);
+    if (screened)
+      CUHC_TRY(st, (launchScreen<Metric, PlainWeight, true>(p, metric, PlainWeight{}, index.kc,
+                                                            stream)));
+    else
+      CUHC_TRY(st, (launchPass<Metric, PlainWeight, true>(p, metric, PlainWeight{}, index.kc,
+                                                          stream)));
     if (timer.start) {
       unsigned long long tilesNow = 0;
       cudaMemcpyAsync(&tilesNow, tiles.get(), sizeof(tilesNow), cudaMemcpyDeviceToHost, stream);

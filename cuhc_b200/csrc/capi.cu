@@ -41,6 +41,9 @@ PassStats gStats;
 
 int currentPruneMode() { return gPruneMode.load(); }
 
+std::atomic<int> gScreenMode{0};
+int currentScreenMode() { return gScreenMode.load(); }
+
 int pairwiseIntoMatrix(const float *points, int n, int d, int metricId, float p, float *out,
                        cudaStream_t s) {
   return withMetric(metricId, p, [&](auto m) {
@@ -309,6 +312,16 @@ int cuhc_set_pruning(int mode) {
   if (mode < kPruneAuto || mode > kPruneNever)
     return kErrorInvalidAlgorithm;
   gPruneMode.store(mode);
+  return 0;
+}
+
+// Tensor-core screening of the all-pairs passes (an addition): 0 auto (on
+// for euclidean / sqeuclidean with d <= 32), 1 on where supported, 2 off.
+// Results are identical in every mode; only the time changes.
+int cuhc_set_screen(int mode) {
+  if (mode < 0 || mode > 2)
+    return kErrorInvalidAlgorithm;
+  gScreenMode.store(mode);
   return 0;
 }
 

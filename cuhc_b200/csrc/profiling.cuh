@@ -13,7 +13,7 @@
 namespace cuhc {
 
 enum TimerKind : int { kTimerKnnPass = 0, kTimerNearestPass = 1, kTimerScreenPass = 2,
-                       kNumTimers = 4 };
+                       kTimerScreenKnnPass = 3, kNumTimers = 4 };
 
 void noteLaunch(int count = 1);
 bool timingEnabled();

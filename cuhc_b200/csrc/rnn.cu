@@ -24,6 +24,7 @@
 
 #include "metrics.cuh"
 #include "passes.cuh"
+#include "screen.cuh"
 
 namespace cuhc {
 
@@ -283,9 +284,14 @@ int rnnWard(const float *devPoints, int n, int d, const RnnOptions &options, dou
     WardWeight w;
     w.value = sizeF[cur].get();
     {
-      PassTimer timer(kTimerNearestPass, s);
-      CUHC_TRY(st, (launchPass<SqEuclideanMetric, WardWeight, false>(p, SqEuclideanMetric{}, w,
-                                                                     index.kc, s)));
+      const bool screened = useScreen<SqEuclideanMetric>(d, 0);
+      PassTimer timer(screened ? kTimerScreenPass : kTimerNearestPass, s);
+      if (screened)
+        CUHC_TRY(st, (launchScreen<SqEuclideanMetric, WardWeight, false>(
+                         p, SqEuclideanMetric{}, w, index.kc, s)));
+      else
+        CUHC_TRY(st, (launchPass<SqEuclideanMetric, WardWeight, false>(p, SqEuclideanMetric{}, w,
+                                                                       index.kc, s)));
       if (timer.start) {
         unsigned long long now = 0;
         cudaMemcpyAsync(&now, tiles.get(), sizeof(now), cudaMemcpyDeviceToHost, s);

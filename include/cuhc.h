@@ -97,6 +97,11 @@ int cuhc_hdbscan_tree_device(const float *devicePoints, int numPoints, int numFe
                              int metricId, float metricParam, int minSamples, float alpha,
                              int coreMethod, double *tree, float *core);
 
+/* Tensor-core screening of the all-pairs passes: 0 auto (on for euclidean and
+ * sqeuclidean up to 32 features), 1 on where supported, 2 off. Results never
+ * change; returns CUHC_ERROR_INVALID_ALGORITHM for other values. */
+int cuhc_set_screen(int mode);
+
 /* Cumulative counters since load: out[0] tiles computed, out[1] tiles in all
  * passes, out[2] passes, out[3] Borůvka rounds (first `count` of them). */
 int cuhc_pass_stats(unsigned long long *out, int count);
@@ -122,7 +127,7 @@ unsigned long long cuhc_launch_count(void);
 int cuhc_set_timing(int on);
 
 /* Per pass kind (0 k-NN pass, 1 nearest-other-component pass, 2 screened
- * pass): device milliseconds, launches and tiles computed since the last
+ * nearest pass, 3 screened k-NN pass): device milliseconds, launches and tiles computed since the last
  * call (first `count` kinds); resets them. */
 int cuhc_kernel_timing(double *ms, unsigned long long *launches, unsigned long long *tiles,
                        int count);
