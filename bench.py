@@ -197,6 +197,8 @@ def main():
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--no-plain", action="store_true",
+                        help="skip the screening-off comparison step")
     parser.add_argument("--n", type=int, default=N_POINTS,
                         help="points of the same recipe (smaller cases for profiling)")
     args = parser.parse_args()
@@ -283,6 +285,14 @@ def main():
     kt = _lib.kernel_timing()
     _lib.set_timing(False)
 
+    # The same step with tensor-core screening switched off (plain FP32 passes).
+    plain = float("nan")
+    if not args.no_plain:
+        _lib.set_screen("off")
+        device_step()
+        plain = float(np.mean(timed(device_step, max(1, min(args.steps, 3)))))
+        _lib.set_screen("auto")
+
     # End to end through the host API (pinned buffers, copies included).
     for _ in range(1):
         host_step()
@@ -290,47 +300,65 @@ def main():
     e2e = float(np.mean(e2e_times))
 
     # Max over ranks.
-    t = torch.tensor([per_step, e2e], device="cuda")
+    t = torch.tensor([per_step, e2e, plain], device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    per_step, e2e = float(t[0]), float(t[1])
+    per_step, e2e, plain = float(t[0]), float(t[1]), float(t[2])
 
     if rank == 0:
         peaks, peak_kind = measured_peaks()
         fp32 = fp32_peak_tflops(torch)
-        knn_ms, knn_launch, knn_tiles = kt["knn_pass"]
-        near_ms, near_launch, near_tiles = kt["nearest_pass"]
-        # Dominant kernel: the pass kind with the most device time. Work per
-        # evaluated pair: 3 d FP32 FLOP (d subtractions + d fused multiply-adds).
+        # Dominant kernel: the pass kind with the most device time.
         kind, (ms, nl, tiles) = max(kt.items(), key=lambda kv: kv[1][0])
-        flops = tiles * 128 * 128 * 3 * d
-        achieved = flops / (ms / 1e3) / 1e12 if ms > 0 else 0.0
+        screened = kind.startswith("screen")
+        pairs = tiles * 128 * 128
+        sgemm = f"cuBLAS SGEMM 8192^3 with TF32 off, measured in this run: {fp32:.2f} TFLOP/s"
+        if screened:
+            # Screened pass: 2d tensor FLOP per evaluated pair (the -2 X Y^T
+            # product) against the TF32 rate, half the measured bf16 burst.
+            peak = peaks["bf16_tflops"] / 2 if peaks.get("bf16_tflops") else None
+            achieved = pairs * 2 * d / (ms / 1e3) / 1e12 if ms > 0 else 0.0
+            k_pad = (3 * d + 4 + 7) // 8 * 8
+            issued = pairs * 2 * k_pad / (ms / 1e3) / 1e12 if ms > 0 else 0.0
+            roof = {"bound": "tensor", "kernel": kind, "achieved": round(achieved, 2),
+                    "peak": round(peak, 1) if peak else None, "unit": "TFLOP/s",
+                    "frac": round(achieved / peak, 4) if peak else None, "traffic": None,
+                    "peak_source": f"TF32 = half the bf16 burst {peaks.get('bf16_tflops')} "
+                                   f"TFLOP/s ({peak_kind})",
+                    "work": f"{tiles} tiles x 16384 pairs x 2d FLOP in {nl} launches, "
+                            f"{ms:.1f} ms",
+                    "issued_tflops": round(issued, 2),
+                    "fp32_equivalent": {"achieved": round(pairs * 3 * d / (ms / 1e3) / 1e12, 2),
+                                        "peak": round(fp32, 2), "peak_source": sgemm}}
+        else:
+            # Plain pass: 3d FP32 FLOP per evaluated pair (d subtractions + d
+            # fused multiply-adds) against the FP32 pipe.
+            achieved = pairs * 3 * d / (ms / 1e3) / 1e12 if ms > 0 else 0.0
+            roof = {"bound": "fp32", "kernel": kind, "achieved": round(achieved, 2),
+                    "peak": round(fp32, 2), "unit": "TFLOP/s",
+                    "frac": round(achieved / fp32, 3) if fp32 else None, "traffic": None,
+                    "peak_source": sgemm,
+                    "work": f"{tiles} tiles x 16384 pairs x 3d FLOP in {nl} launches, "
+                            f"{ms:.1f} ms"}
         line = {
             "metric": METRIC, "value": round(per_step, 4), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 2),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": f"hdbscan {n:,} x 8, 20 blobs + 10% noise, min_samples 25",
-                       "n": n, "d": d, "min_samples": MIN_SAMPLES, "path": "plain exact fp32",
+                       "n": n, "d": d, "min_samples": MIN_SAMPLES,
+                       "path": "tcgen05 TF32 screen + exact FP32 recheck" if screened
+                               else "plain exact fp32",
                        "l2": "flushed before every step (256 MB write)",
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": int(X.nbytes),
                     "d2h_bytes_per_step": int((n - 1) * 4 * 8 + n * 4)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "fp32", "kernel": kind, "achieved": round(achieved, 2),
-                         "peak": round(fp32, 2), "unit": "TFLOP/s",
-                         "frac": round(achieved / fp32, 3) if fp32 else None,
-                         "traffic": None,
-                         "peak_source": "cuBLAS SGEMM 8192^3 with TF32 off, measured in this run "
-                                        "(the plain pass runs on the FP32 pipe); "
-                                        f"bf16 tensor peak {peaks.get('bf16_tflops')} TFLOP/s "
-                                        f"({peak_kind})",
-                         "work": f"{tiles} tiles x 16384 pairs x 3d FLOP in {nl} launches, "
-                                 f"{ms:.1f} ms"},
-            "passes": {"knn": {"ms": round(knn_ms, 2), "launches": knn_launch,
-                               "tiles": knn_tiles},
-                       "nearest": {"ms": round(near_ms, 2), "launches": near_launch,
-                                   "tiles": near_tiles},
+            "roofline": roof,
+            "plain_fp32": {"value": None if np.isnan(plain) else round(plain, 4), "unit": UNIT,
+                           "note": "same step with tensor-core screening off"},
+            "passes": {**{k: {"ms": round(v[0], 2), "launches": v[1], "tiles": v[2]}
+                          for k, v in kt.items()},
                        "tiles_per_step": int((stats1[0] - stats0[0]) / max(args.steps, 1)),
                        "rounds_per_step": (stats1[3] - stats0[3]) / max(args.steps, 1)},
             "clocks": clocks.summary(),

@@ -40,6 +40,28 @@ __device__ __forceinline__ void mbarrierArriveExpectTx(uint64_t *bar, uint32_t b
                : "memory");
 }
 
+// Plain arrival of `count` on the barrier, releasing this thread's earlier
+// shared-memory writes to the threads that wait on the phase.
+__device__ __forceinline__ void mbarrierArrive(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddress(bar)),
+               "r"(count)
+               : "memory");
+}
+
+// Named barrier `id` over `threads` threads (a multiple of 32) that also ORs a
+// predicate across them: every participant gets the same answer.
+__device__ __forceinline__ bool namedBarrierOr(int id, int threads, bool predicate) {
+  uint32_t out;
+  asm volatile("{\n\t.reg .pred p, q;\n\t"
+               "setp.ne.u32 p, %1, 0;\n\t"
+               "bar.red.or.pred q, %2, %3, p;\n\t"
+               "selp.u32 %0, 1, 0, q;\n\t}"
+               : "=r"(out)
+               : "r"((uint32_t)predicate), "r"(id), "r"(threads)
+               : "memory");
+  return out != 0;
+}
+
 __device__ __forceinline__ void bulkCopyToShared(void *dst, const void *src, uint32_t bytes,
                                                  uint64_t *bar) {
   asm volatile(
@@ -60,12 +82,28 @@ __device__ __forceinline__ bool mbarrierTryWait(uint64_t *bar, uint32_t phase) {
   return done != 0;
 }
 
-// Waits for the barrier's phase `phase` to complete; false if the iteration
-// limit ran out first.
+__device__ __forceinline__ uint64_t globalTimerNs() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// A wait on a copy or an MMA that has not completed after this long never
+// will: the kernel records kErrorTimeout and leaves.
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
+
+// Waits for the barrier's phase `phase` to complete; false if a second of
+// wall-clock time (or the iteration limit) ran out first.
 __device__ __forceinline__ bool mbarrierWait(uint64_t *bar, uint32_t phase) {
-  for (long long spins = 0; spins < kSpinLimit; ++spins)
+  if (mbarrierTryWait(bar, phase))
+    return true;
+  const uint64_t start = globalTimerNs();
+  for (long long spins = 0; spins < kSpinLimit; ++spins) {
     if (mbarrierTryWait(bar, phase))
       return true;
+    if ((spins & 63) == 63 && globalTimerNs() - start > kWaitLimitNs)
+      return false;
+  }
   return false;
 }
 

@@ -204,6 +204,7 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
   p.tilesComputed = tiles.get();
   p.error = error.get();
 
+  const bool screened = useScreen<Metric>(index.d, 0) && index.extentsWithin(kScreenMaxExtent);
   int numComponents = n, totalEdges = 0, rounds = 0;
   unsigned long long tilesSoFar = 0;
   int hostCounters[4];
@@ -218,7 +219,6 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
     CUHC_TRY(st, cudaGetLastError());
     p.singletons = rounds == 0;
     {
-      const bool screened = useScreen<Metric>(index.d, 0);
       PassTimer timer(screened ? kTimerScreenPass : kTimerNearestPass, stream);
       if (screened)
         CUHC_TRY(st, (launchScreen<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
@@ -252,12 +252,19 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
     countRoots<<<blocks(n), 256, 0, stream>>>(comp.get(), parent.get(), counters.get(), n); noteLaunch();
     relabel<<<blocks(n), 256, 0, stream>>>(comp.get(), parent.get(), n); noteLaunch();
     CUHC_TRY(st, cudaGetLastError());
+    int passError = 0;
     CUHC_TRY(st, cudaMemcpyAsync(hostCounters, counters.get(), 4 * sizeof(int),
                                  cudaMemcpyDeviceToHost, stream));
+    CUHC_TRY(st, cudaMemcpyAsync(&passError, error.get(), sizeof(int), cudaMemcpyDeviceToHost,
+                                 stream));
     CUHC_TRY(st, cudaStreamSynchronize(stream));
     if (!st.ok())
       break;
     ++rounds;
+    if (passError != 0) {
+      st(passError);
+      break;
+    }
     const int added = hostCounters[0];
     if (hostCounters[2] != 0) {
       st(kErrorTimeout);
@@ -326,7 +333,8 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
   p.tilesComputed = tiles.get();
   p.error = error.get();
   {
-    const bool screened = useScreen<Metric>(index.d, k);
+    const bool screened =
+        useScreen<Metric>(index.d, k) && index.extentsWithin(kScreenMaxExtent);
     PassTimer timer(screened ? kTimerScreenKnnPass : kTimerKnnPass, stream);
     if (screened)
       CUHC_TRY(st, (launchScreen<Metric, PlainWeight, true>(p, metric, PlainWeight{}, index.kc,

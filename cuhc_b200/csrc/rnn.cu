@@ -284,7 +284,8 @@ int rnnWard(const float *devPoints, int n, int d, const RnnOptions &options, dou
     WardWeight w;
     w.value = sizeF[cur].get();
     {
-      const bool screened = useScreen<SqEuclideanMetric>(d, 0);
+      const bool screened =
+          useScreen<SqEuclideanMetric>(d, 0) && index.extentsWithin(kScreenMaxExtent);
       PassTimer timer(screened ? kTimerScreenPass : kTimerNearestPass, s);
       if (screened)
         CUHC_TRY(st, (launchScreen<SqEuclideanMetric, WardWeight, false>(
@@ -311,11 +312,16 @@ int rnnWard(const float *devPoints, int n, int d, const RnnOptions &options, dou
         mergeU.get(), mergeV.get(), mergeH.get(), counter.get(), n - 1);
     noteLaunch();
     CUHC_TRY(st, cudaGetLastError());
-    int total = 0;
+    int total = 0, passError = 0;
     CUHC_TRY(st, cudaMemcpyAsync(&total, counter.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUHC_TRY(st, cudaMemcpyAsync(&passError, error.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     CUHC_TRY(st, cudaStreamSynchronize(s));
     if (!st.ok())
       break;
+    if (passError != 0) {
+      st(passError);
+      break;
+    }
     ++rounds;
     const int roundMerges = total - merged;
     merged = total;

@@ -1,30 +1,49 @@
-// The tensor-core screened pass: the same nearest / k-NN passes as
-// passes.cuh, with the all-pairs distance work moved to tcgen05 MMAs.
+// The tensor-core screened pass: the nearest / k-NN passes of passes.cuh
+// with the all-pairs distance work moved to tcgen05 MMAs.
 //
-// Per row tile the block centres every point on the row tile's box centre c
-// and builds TF32 operands (K-major, shared memory) such that one
-// accumulation over K = 3d + 4 (padded to 8) gives, in tensor memory,
-//   D'(i, j) = (1 - e) n_i + (1 - e) n_j - 2 (xh.yh + xh.yl + xl.yh)
-// where x = x_i - c = xh + xl and y = y_j - c = yh + yl are TF32 splits and
-// n = |x|^2. The margin e (screenMargin) is twice a rigorous bound of every
-// error involved, as a multiple of n_i + n_j: the TF32 splits, the dropped
-// xl.yl term, the norms' FP32 rounding, the centring rounding, the tensor
-// core's FP32 accumulation (modelled pessimistically: every addition off by
-// 2^-22 of the sum of absolute products, four times over), and the
-// reference's own FP32 rounding of the exact squared distance s. Hence
-// D'(i, j) <= s(i, j) for every pair, and a pair can only pass its row's
-// filter bound F (a bound on s) if D'(i, j) <= F. Exactly those pairs are
-// recomputed with the reference's FP32 fmaf chain from the raw features, so
-// every weight, key and k-th distance is bit-identical to the plain pass.
+// Screen. Per row tile the block centres every coordinate on the row tile's
+// box centre c (x = a - c, y = b - c, FP32) and builds K-major TF32 operands
+// such that one MMA accumulation gives, in tensor memory,
+//     D'(i, j) = N_i + N_j - 2 sum_k tf32(x_k) tf32(y_k)   (+ 2^90, below)
+// with N = (1 - e) |x|^2 split into two TF32 terms. The margin e
+// (screenMargin) is twice a rigorous bound, as a multiple of |x|^2 + |y|^2,
+// of every error involved: the one-term TF32 product (2^-10), the norms' FP32
+// rounding and split, the centring rounding, the tensor core's FP32
+// accumulation (modelled as 2^-22 of the sum of absolute products per
+// addition, four times over) and the reference's own FP32 rounding of the
+// squared distance s. Hence D'(i, j) <= s(i, j) for every pair of different
+// components, and a pair can only pass its row's filter bound F (a bound on
+// s) if D'(i, j) <= F + 2^-70 (the absolute term covers subnormal products
+// that the tensor core may flush). Exactly those pairs are recomputed with
+// the reference's FP32 chain from the raw coordinates, so every weight, key
+// and k-th distance is bit-identical to the plain pass. The screen needs
+// every coordinate extent <= 2^40 (nothing overflows); wider data runs plain.
 //
-// Roles per column tile: warps 4-7 build the column operand (one column per
-// thread), thread 0 issues the MMAs and commits them to an mbarrier, warps
-// 0-3 read the accumulator (one row per thread: tensor-memory lane = row),
-// take the row minimum of D' and recheck only the rows that have a pair at or
-// below the filter bound. Candidate collection, nearest-first order and the
-// bulk-copy double buffering are those of passes.cuh.
+// Component indicators. In Borůvka rounds a row's own component must not
+// count. When the row tile holds at most R distinct components (R = the K
+// slots left after coordinates and norms, >= 4), slot q of row i holds 2^90
+// if comp(i) is the q-th of them and slot q of column j holds 1 if comp(j)
+// is: the MMA adds 2^90 to every same-component pair and exactly 0 to every
+// other pair, and the epilogue takes a plain row minimum. Otherwise the
+// epilogue masks by component.
+//
+// Pipeline, warp-specialised, one row tile per block:
+//   producer warps 4-7 (column j = thread - 128): build the column operand of
+//     each staged column tile; thread 128 also issues the bulk copies (raw
+//     coordinates + metadata, a ring of four, two ahead) and the MMAs;
+//   consumer warps 0-3 (row i = thread = tensor-memory lane): read the
+//     accumulator, take the row minimum, recheck rows with a pair at or below
+//     their filter, refresh the row threshold.
+// Tensor memory holds two 128 x 128 FP32 accumulators, so the producers
+// build and multiply tile t + 1 while the consumers read tile t. mbarriers
+// link the stages: rawFull (copy landed), mmaFull (MMA done + slot info),
+// tmemEmpty / rawEmpty (consumers done). Candidate collection and ordering
+// are those of passes.cuh, one batch at a time; a sentinel ends each batch.
+// Every wait is bounded; one that runs out stops both groups at the same
+// ordinal and the pass returns kErrorTimeout.
 #pragma once
 
+#include <climits>
 #include <cmath>
 
 #include "passes.cuh"
@@ -32,94 +51,155 @@
 
 namespace cuhc {
 
-__host__ __device__ inline int screenK(int d) { return (3 * d + 4 + 7) / 8 * 8; }
+// K of the screened product for chunk width KC: KC coordinates, 4 norm
+// terms and at least 4 component slots, a multiple of the MMA's K step (8).
+__host__ __device__ constexpr int screenKPad(int kc) { return (kc + 8 + 7) / 8 * 8; }
+__host__ __device__ constexpr int screenSlots(int kc) { return screenKPad(kc) - kc - 4; }
+constexpr int kScreenStages = 4; // column tiles staged in shared memory
+constexpr int kScreenAhead = 2;  // copies issued ahead of the tile being built
+constexpr int kScreenMaxSlots = 8;
+constexpr float kIndicator = 0x1p90f;
+constexpr float kScreenAbsSlack = 0x1p-70f;
+constexpr float kScreenMaxExtent = 0x1p40f;
 
-// e: see the header comment. Units of n_i + n_j.
-inline float screenMargin(int d) {
-  const double u22 = std::ldexp(1.0, -22), u24 = std::ldexp(1.0, -24);
-  const int K = screenK(d);
-  const double mma = 4.0 * (9.0 * K / 8.0) * 2.02 * u22;     // accumulation, four times over
-  const double split = 3.0 * u22;                             // TF32 splits, dropped lo*lo
-  const double norm = ((d + 1) / 4.0 + 1.25) * u22;           // norms, scaling, their split
-  const double centre = u22;                                  // rounding of x - c
-  const double reference = 2.01 * (d + 1) * u24 * 1.01;       // the exact fmaf chain itself
-  return (float)(2.0 * (mma + split + norm + centre + reference));
+// e of the header comment, for d features staged as chunks of kc.
+inline float screenMargin(int d, int kc) {
+  const double u = std::ldexp(1.0, -24), t = std::ldexp(1.0, -11), u22 = std::ldexp(1.0, -22);
+  const double product = t * (2.0 + t);                 // tf32(x) tf32(y) against x y
+  const double norms = 1.01 * kc * u + u + u22;         // |x|^2 in FP32, times (1 - e), split
+  const double mma = 4.0 * screenKPad(kc) * u22 * 2.01; // accumulation, four times over
+  const double centring = 4.0 * u;                      // a - c and b - c rounded
+  const double reference = 2.02 * (d + 3) * u;          // the reference's FP32 chain
+  return (float)(2.0 * (product + norms + mma + centring + reference));
 }
 
-// Warps 4-7 (column j = tid - 128): TF32 operand row of column j of a staged
-// raw tile, centred on c.
-__device__ __forceinline__ void buildColumnOperand(const float *raw, const float *centre, int d,
-                                                   int kPad, float scale, float *op,
-                                                   uint32_t sbo, int j) {
-  char *base = reinterpret_cast<char *>(op);
+// Dynamic shared memory of a screened block, in floats from the base.
+template <int KC> struct ScreenLayout {
+  static constexpr int kPad = screenKPad(KC);
+  static constexpr size_t rawFloats = (size_t)KC * kTile;
+  static constexpr size_t metaInts = 3 * kTile; // orig, comp, value
+  static constexpr size_t sA = 0;
+  static constexpr size_t raw = sA + rawFloats;
+  static constexpr size_t meta = raw + kScreenStages * rawFloats;
+  static constexpr size_t opA = meta + kScreenStages * metaInts;
+  static constexpr size_t opB = opA + (size_t)kTile * kPad;
+  static constexpr size_t box = opB + 2 * (size_t)kTile * kPad; // low, high, centre (KC each)
+  static constexpr size_t lists = box + 3 * KC;
+  static size_t bytes(int k) { return (lists + (size_t)kTile * k) * sizeof(float); }
+};
+
+struct ScreenSync {
+  uint64_t rawFull[kScreenStages], rawEmpty[kScreenStages];
+  uint64_t mmaFull[2], tmemEmpty[2];
+  int rawTile[kScreenStages]; // column tile (| kPureColumnTile) per ring slot, -1 ends the batch
+  int slotTile[2];            // the same, per accumulator
+  float warpThr[4];
+  int rowSet[kScreenMaxSlots];
+  int rowSetCount, oneHot, failed;
+  uint32_t tmemBase;
+};
+
+__device__ __forceinline__ float min3(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
+// Bounded wait that gives up at once when the block already failed; false
+// when it did not see the phase complete.
+__device__ __forceinline__ bool screenWait(uint64_t *bar, uint32_t parity, ScreenSync &ss) {
+  if (*(volatile int *)&ss.failed)
+    return false;
+  if (mbarrierWait(bar, parity))
+    return true;
+  *(volatile int *)&ss.failed = 1;
+  return false;
+}
+
+// Stores the kPad operand values of one point (row of the K-major canonical
+// layout: 8-row core matrices of 16-byte rows, LBO 128, SBO kPad * 32).
+template <int kPad>
+__device__ __forceinline__ void storeOperandRow(float *op, int row, const float (&val)[kPad]) {
+  char *base = reinterpret_cast<char *>(op) + (size_t)(row >> 3) * (kPad * 32) + (row & 7) * 16;
+#pragma unroll
+  for (int q = 0; q < kPad / 4; ++q)
+    *reinterpret_cast<float4 *>(base + q * 128) =
+        make_float4(val[4 * q], val[4 * q + 1], val[4 * q + 2], val[4 * q + 3]);
+}
+
+// Row operand of row tile point i: [x (KC), N hi, N lo, 1, 1, indicators].
+template <int KC>
+__device__ __forceinline__ void buildRowOperand(const float *sA, const float *centre, float scale,
+                                                int i, bool valid, int comp,
+                                                const ScreenSync &ss, float *opA) {
+  constexpr int kPad = screenKPad(KC), R = screenSlots(KC);
+  float val[kPad];
   float n = 0.0f;
-  for (int k = 0; k < d; ++k) {
+#pragma unroll
+  for (int k = 0; k < KC; ++k) {
+    const float x = sA[k * kTile + i] - centre[k];
+    n = fmaf(x, x, n);
+    val[k] = toTf32(x);
+  }
+  const float ns = n * scale, nh = toTf32(ns);
+  val[KC] = nh;
+  val[KC + 1] = toTf32(ns - nh);
+  val[KC + 2] = 1.0f;
+  val[KC + 3] = 1.0f;
+#pragma unroll
+  for (int q = 0; q < R; ++q)
+    val[KC + 4 + q] =
+        (ss.oneHot && valid && q < ss.rowSetCount && comp == ss.rowSet[q]) ? kIndicator : 0.0f;
+  storeOperandRow<kPad>(opA, i, val);
+}
+
+// Column operand of staged point j: [-2 y (KC), 1, 1, N hi, N lo, indicators].
+template <int KC>
+__device__ __forceinline__ void buildColumnOperand(const float *raw, const int *comp,
+                                                   const float *centre, float scale, int j,
+                                                   bool oneHot, const ScreenSync &ss,
+                                                   float *opB) {
+  constexpr int kPad = screenKPad(KC), R = screenSlots(KC);
+  float val[kPad];
+  float n = 0.0f;
+#pragma unroll
+  for (int k = 0; k < KC; ++k) {
     const float y = raw[k * kTile + j] - centre[k];
     n = fmaf(y, y, n);
-    const float hi = toTf32(y), lo = toTf32(y - hi);
-    *reinterpret_cast<float *>(base + umma_offset(j, k, sbo)) = -2.0f * hi;
-    *reinterpret_cast<float *>(base + umma_offset(j, d + k, sbo)) = -2.0f * lo;
-    *reinterpret_cast<float *>(base + umma_offset(j, 2 * d + k, sbo)) = -2.0f * hi;
+    val[k] = -2.0f * toTf32(y);
   }
-  const float ns = n * scale;
-  const float nh = toTf32(ns), nl = toTf32(ns - nh);
-  *reinterpret_cast<float *>(base + umma_offset(j, 3 * d, sbo)) = 1.0f;
-  *reinterpret_cast<float *>(base + umma_offset(j, 3 * d + 1, sbo)) = 1.0f;
-  *reinterpret_cast<float *>(base + umma_offset(j, 3 * d + 2, sbo)) = nh;
-  *reinterpret_cast<float *>(base + umma_offset(j, 3 * d + 3, sbo)) = nl;
-  for (int k = 3 * d + 4; k < kPad; ++k)
-    *reinterpret_cast<float *>(base + umma_offset(j, k, sbo)) = 0.0f;
-}
-
-// Threads 0..127 (row i = tid): the row operand (built once per block).
-__device__ __forceinline__ void buildRowOperand(const float *raw, const float *centre, int d,
-                                                int kPad, float scale, float *op, uint32_t sbo,
-                                                int i) {
-  char *base = reinterpret_cast<char *>(op);
-  float n = 0.0f;
-  for (int k = 0; k < d; ++k) {
-    const float x = raw[k * kTile + i] - centre[k];
-    n = fmaf(x, x, n);
-    const float hi = toTf32(x), lo = toTf32(x - hi);
-    *reinterpret_cast<float *>(base + umma_offset(i, k, sbo)) = hi;
-    *reinterpret_cast<float *>(base + umma_offset(i, d + k, sbo)) = hi;
-    *reinterpret_cast<float *>(base + umma_offset(i, 2 * d + k, sbo)) = lo;
-  }
-  const float ns = n * scale;
-  const float nh = toTf32(ns), nl = toTf32(ns - nh);
-  *reinterpret_cast<float *>(base + umma_offset(i, 3 * d, sbo)) = nh;
-  *reinterpret_cast<float *>(base + umma_offset(i, 3 * d + 1, sbo)) = nl;
-  *reinterpret_cast<float *>(base + umma_offset(i, 3 * d + 2, sbo)) = 1.0f;
-  *reinterpret_cast<float *>(base + umma_offset(i, 3 * d + 3, sbo)) = 1.0f;
-  for (int k = 3 * d + 4; k < kPad; ++k)
-    *reinterpret_cast<float *>(base + umma_offset(i, k, sbo)) = 0.0f;
+  const float ns = n * scale, nh = toTf32(ns);
+  val[KC] = 1.0f;
+  val[KC + 1] = 1.0f;
+  val[KC + 2] = nh;
+  val[KC + 3] = toTf32(ns - nh);
+  const int c = oneHot ? comp[j] : INT_MIN;
+#pragma unroll
+  for (int q = 0; q < R; ++q)
+    val[KC + 4 + q] = (oneHot && q < ss.rowSetCount && c == ss.rowSet[q]) ? 1.0f : 0.0f;
+  storeOperandRow<kPad>(opB, j, val);
 }
 
 template <class Metric, class Weight, int KC, bool kKnn>
 __global__ void __launch_bounds__(kThreads, 2)
-    screenKernel(PassParams p, Metric m, Weight w, float margin, int kPad) {
+    screenKernel(PassParams p, Metric m, Weight w, float margin) {
+  using L = ScreenLayout<KC>;
+  constexpr int kPad = L::kPad;
+  constexpr uint32_t kSbo = kPad * 32;
+  constexpr int R = screenSlots(KC);
   extern __shared__ __align__(128) float dyn[];
   __shared__ PassState sh;
-  __shared__ uint64_t mmaBar;
-  __shared__ uint32_t tmemBase;
-  float *sA = dyn;
-  float *sB[2] = {sA + KC * kTile, sA + 2 * KC * kTile};
-  int *metaBase = (int *)(sA + 3 * KC * kTile);
-  ColumnMeta meta[2];
-  for (int b = 0; b < 2; ++b) {
-    meta[b].orig = metaBase + b * 3 * kTile;
-    meta[b].comp = metaBase + b * 3 * kTile + kTile;
-    meta[b].value = (float *)(metaBase + b * 3 * kTile + 2 * kTile);
-  }
-  float *opA = (float *)(metaBase + 6 * kTile);
-  float *opB = opA + kTile * kPad;
-  float *rowLow = opB + kTile * kPad;
-  float *rowHigh = rowLow + p.d;
-  float *centre = rowHigh + p.d;
-  float *lists = centre + p.d;
-  const uint32_t sbo = (uint32_t)kPad * 32u;
+  __shared__ ScreenSync ss;
+  float *sA = dyn + L::sA;
+  float *rawBase = dyn + L::raw;
+  int *metaBase = reinterpret_cast<int *>(dyn + L::meta);
+  float *opA = dyn + L::opA, *opB = dyn + L::opB;
+  float *rowLow = dyn + L::box, *rowHigh = rowLow + KC, *centre = rowHigh + KC;
+  float *lists = dyn + L::lists;
 
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool consumer = tid < kTile;
+  const bool leader = tid == kTile;
   const int I = blockIdx.x;
   const int firstRow = I * kTile;
   const int leaf = p.leafOfTile[I];
@@ -128,36 +208,49 @@ __global__ void __launch_bounds__(kThreads, 2)
   const float slack = 1.0f - boxSlack(p.d);
   const bool useComp = !kKnn && p.component != nullptr;
   const bool useValue = !kKnn && w.value != nullptr;
-  const size_t tileFloats = (size_t)KC * kTile; // one chunk: d <= 32
   const float scale = 1.0f - margin;
 
-  // Epilogue threads own one row each.
+  // Consumer row state (thread = row).
   const int myRow = tid & (kTile - 1);
   const int myPos = firstRow + myRow;
-  const bool myValid = myPos < p.n;
+  const bool myValid = consumer && myPos < p.n;
   const int myComp = myValid ? (p.component ? p.component[myPos] : p.order[myPos]) : -2;
   const float myVal = myValid ? w.load(myPos) : 0.0f;
+  unsigned int *compSlot = (!kKnn && myValid && p.compBest) ? p.compBest + myComp : nullptr;
 
-  if (tid < kTile)
-    sh.rowBest[tid] = kEmptyKey;
   if (kKnn)
     for (int i = tid; i < kTile * p.k; i += kThreads)
       lists[i] = INFINITY;
-  for (int f = tid; f < p.d; f += kThreads) {
-    rowLow[f] = p.nodeLow[(size_t)leaf * p.d + f];
-    rowHigh[f] = p.nodeHigh[(size_t)leaf * p.d + f];
-    centre[f] = 0.5f * (rowLow[f] + rowHigh[f]);
+  for (int f = tid; f < KC; f += kThreads) {
+    const bool real = f < p.d;
+    const float lo = real ? p.nodeLow[(size_t)leaf * p.d + f] : 0.0f;
+    const float hi = real ? p.nodeHigh[(size_t)leaf * p.d + f] : 0.0f;
+    rowLow[f] = lo;
+    rowHigh[f] = hi;
+    centre[f] = real ? 0.5f * (lo + hi) : 0.0f;
   }
-  copyChunk(sA, p.tiled + (size_t)I * tileFloats, KC * kTile);
+  copyChunk(sA, p.tiled + (size_t)I * L::rawFloats, KC * kTile);
   if (warp == 0) {
-    tmemAlloc(&tmemBase, kTile);
+    tmemAlloc(&ss.tmemBase, 256);
     tmemRelinquish();
   }
+  const bool wantOneHot = !kKnn && useComp && !p.singletons;
+  int *rowComps = metaBase; // ring slot 0 is free until the first copy
+  if (consumer && wantOneHot)
+    rowComps[myRow] = myValid ? myComp : -1;
   if (tid == 0) {
-    mbarrierInit(&sh.bar[0], 1);
-    mbarrierInit(&sh.bar[1], 1);
-    mbarrierInit(&mmaBar, 1);
+    for (int s = 0; s < kScreenStages; ++s) {
+      mbarrierInit(&ss.rawFull[s], 1);
+      mbarrierInit(&ss.rawEmpty[s], 1);
+    }
+    for (int s = 0; s < 2; ++s) {
+      mbarrierInit(&ss.mmaFull[s], 2); // the MMA commit + the issuer's release of slotTile
+      mbarrierInit(&ss.tmemEmpty[s], 1);
+    }
     fenceBarrierInit();
+    ss.failed = 0;
+    ss.oneHot = 0;
+    ss.rowSetCount = 0;
     sh.frontLen = 0;
     sh.overflow = 0;
     const int rootPure = (!kKnn && p.nodePure) ? p.nodePure[0] : -1;
@@ -166,214 +259,313 @@ __global__ void __launch_bounds__(kThreads, 2)
       sh.frontLen = 1;
     }
   }
-  if (tid < kTile) {
-    const int pos = firstRow + tid;
-    const bool valid = pos < p.n;
-    meta[0].orig[tid] = valid ? p.order[pos] : -1;
-    if (useComp)
-      meta[0].comp[tid] = valid ? p.component[pos] : -1;
-    if (useValue)
-      meta[0].value[tid] = valid ? w.load(pos) : 0.0f;
+  __syncthreads();
+  if (wantOneHot && tid == 0) {
+    // Distinct components of the row tile, up to R.
+    int count = 0;
+    bool ok = true;
+    for (int i = 0; i < kTile && ok; ++i) {
+      const int c = rowComps[i];
+      if (c < 0)
+        continue;
+      bool found = false;
+      for (int q = 0; q < count; ++q)
+        found |= ss.rowSet[q] == c;
+      if (!found) {
+        if (count == R)
+          ok = false;
+        else
+          ss.rowSet[count++] = c;
+      }
+    }
+    ss.rowSetCount = count;
+    ss.oneHot = ok ? 1 : 0;
   }
   __syncthreads();
   tcgenFenceAfter();
-  const uint32_t tmem = tmemBase;
-  if (tid < kTile)
-    buildRowOperand(sA, centre, p.d, kPad, scale, opA, sbo, tid);
+  const uint32_t tmem = ss.tmemBase;
+  const bool oneHot = ss.oneHot != 0;
+  if (consumer)
+    buildRowOperand<KC>(sA, centre, scale, myRow, myValid, myComp, ss, opA);
   fenceProxyAsync();
-  __syncthreads();
-  refreshThresholds<Metric, Weight, kKnn>(p, m, w, sh, lists, firstRow);
 
-  unsigned long long computed = 0;
-  bool failed = false;
-  uint32_t mmaPhase = 0;
+  // Row threshold: sets F (the row's filter bound) and returns the row's
+  // threshold for the block maximum (-inf for rows that can gain nothing).
+  unsigned long long rowBest = kEmptyKey;
+  float F = -INFINITY;
+  auto refresh = [&](unsigned int cb) -> float {
+    float thr;
+    if (kKnn) {
+      thr = lists[myRow * p.k + p.k - 1];
+      F = myValid ? m.filterBound(thr) : -INFINITY;
+    } else {
+      thr = rowBest == kEmptyKey ? INFINITY : keyWeight(rowBest);
+      if (compSlot) {
+        if (rowBest != kEmptyKey && floatBits(thr) < cb)
+          cb = min(cb, atomicMin(compSlot, floatBits(thr)));
+        thr = fminf(thr, bitsFloat(cb));
+      }
+      F = (myValid && w.feasible(thr, myVal)) ? m.filterBound(w.distBound(thr, myVal))
+                                              : -INFINITY;
+    }
+    return F == -INFINITY ? -INFINITY : thr;
+  };
+  auto warpMaxThr = [&](float t) {
+#pragma unroll
+    for (int off = 16; off > 0; off /= 2)
+      t = fmaxf(t, __shfl_xor_sync(0xffffffffu, t, off));
+    if (lane == 0)
+      ss.warpThr[warp] = t;
+  };
+  if (consumer)
+    warpMaxThr(refresh(compSlot ? __ldcg(compSlot) : 0xffffffffu));
+  __syncthreads();
+  if (tid == 0)
+    sh.thrTile = fmaxf(fmaxf(ss.warpThr[0], ss.warpThr[1]), fmaxf(ss.warpThr[2], ss.warpThr[3]));
+  __syncthreads();
+
   const uint32_t idesc = umma_idesc_tf32(128, 128);
   const bool maskPass = useComp && !p.singletons;
-
-  // One staged column tile: operand, MMA, screened epilogue.
-  auto processTile = [&](int J, const float *raw, const ColumnMeta &cm, bool colPure) {
-    if (tid >= kTile)
-      buildColumnOperand(raw, centre, p.d, kPad, scale, opB, sbo, tid - kTile);
-    fenceProxyAsync();
-    __syncthreads();
-    if (tid == 0) {
-      tcgenFenceAfter();
-      for (int s = 0; s < kPad / 8; ++s)
-        mmaTf32(tmem, umma_smem_desc((const char *)opA + 256 * s, 128, sbo),
-                umma_smem_desc((const char *)opB + 256 * s, 128, sbo), idesc, s > 0);
-      mmaCommit(&mmaBar);
-    }
-    const bool done = mbarrierWait(&mmaBar, mmaPhase);
-    mmaPhase ^= 1;
-    if (__syncthreads_or(!done)) {
-      failed = true;
-      return;
-    }
-    tcgenFenceAfter();
-    if (tid < kTile) {
-      const bool mask = maskPass && !(rowPure >= 0 && colPure);
-      const uint32_t lane = tmem + ((uint32_t)(warp * 32) << 16);
-      float F = sh.rowFilter[myRow];
-      float mn = INFINITY;
-      float v[32];
-#pragma unroll
-      for (int chunk = 0; chunk < 4; ++chunk) {
-        tmemLoad32(lane + chunk * 32, v);
-        if (mask) {
-#pragma unroll
-          for (int c = 0; c < 32; ++c)
-            mn = fminf(mn, cm.comp[chunk * 32 + c] != myComp ? v[c] : INFINITY);
-        } else {
-#pragma unroll
-          for (int c = 0; c < 32; ++c)
-            mn = fminf(mn, v[c]);
-        }
-      }
-      if (__any_sync(0xffffffffu, myValid && mn <= F)) {
-        unsigned long long best = kEmptyKey;
-#pragma unroll 1
-        for (int chunk = 0; chunk < 4; ++chunk) {
-          tmemLoad32(lane + chunk * 32, v);
-          if (!(myValid && mn <= F))
-            continue;
-          unsigned candidates = 0;
-#pragma unroll
-          for (int c = 0; c < 32; ++c)
-            candidates |= (v[c] <= F ? 1u : 0u) << c;
-          while (candidates) {
-            const int c = __ffs(candidates) - 1;
-            candidates &= candidates - 1;
-            const int j = chunk * 32 + c;
-            if (J * kTile + j >= p.n)
-              continue;
-            const int colComp = useComp ? cm.comp[j] : cm.orig[j];
-            if (!kKnn && colComp == myComp)
-              continue;
-            // The reference's exact FP32 distance of the pair.
-            typename Metric::Acc acc = m.init();
-            for (int k = 0; k < p.d; ++k)
-              acc = m.accumulate(acc, sA[k * kTile + myRow], raw[k * kTile + j]);
-            if (kKnn) {
-              const float value =
-                  J * kTile + j == myPos ? 0.0f : fmaxf(m.finalize(acc), 0.0f);
-              float *list = lists + myRow * p.k;
-              insertSorted(list, p.k, value);
-              F = m.filterBound(list[p.k - 1]);
-            } else {
-              const float weight = w.weight(m.finalize(acc), myVal, useValue ? cm.value[j] : 0.0f);
-              if (weight < INFINITY) {
-                const unsigned long long key = packKey(weight, (uint32_t)cm.orig[j]);
-                best = key < best ? key : best;
-              }
-            }
-          }
-        }
-        if (!kKnn && best < sh.rowBest[myRow])
-          sh.rowBest[myRow] = best;
-      }
-    }
-    tcgenFenceBefore();
-    __syncthreads();
-    refreshThresholds<Metric, Weight, kKnn>(p, m, w, sh, lists, firstRow);
-    ++computed;
-  };
-
-  if (rowPure < 0)
-    processTile(I, sA, meta[0], false);
-
   const uint32_t metaBytes = (uint32_t)(kTile * sizeof(int)) * (1 + useComp + useValue);
-  const uint32_t tileBytes = (uint32_t)(KC * kTile * sizeof(float));
-  auto issue = [&](int i, int b) {
-    const int J = sh.listTile[i] & ~kPureColumnTile;
-    fenceProxyAsync();
-    mbarrierArriveExpectTx(&sh.bar[b], tileBytes + metaBytes);
-    bulkCopyToShared(sB[b], p.tiled + (size_t)J * tileFloats, tileBytes, &sh.bar[b]);
-    bulkCopyToShared(meta[b].orig, p.order + (size_t)J * kTile, kTile * sizeof(int), &sh.bar[b]);
-    if (useComp)
-      bulkCopyToShared(meta[b].comp, p.component + (size_t)J * kTile, kTile * sizeof(int),
-                       &sh.bar[b]);
-    if (useValue)
-      bulkCopyToShared(meta[b].value, w.value + (size_t)J * kTile, kTile * sizeof(float),
-                       &sh.bar[b]);
-  };
-  uint32_t phase[2] = {0, 0};
-  bool inFlight[2] = {false, false};
+  const uint32_t tileBytes = (uint32_t)(L::rawFloats * sizeof(float));
+  int t = 0;      // ordinal of tiles and sentinels through the rings (all threads agree)
+  int issued = 0; // leader: ordinals issued
+  int lastCommit = -1;
+  unsigned long long computed = 0;
+  bool selfPending = kKnn || rowPure < 0;
+  bool overflow = false;
 
-  while (!failed) {
-    if (tid < 32)
+  while (true) {
+    if (warp == 0)
       collectCandidates(p, m, w, sh, rowLow, rowHigh, I, rowPure, rowMinValue, slack);
     __syncthreads();
     const int len = sh.listLen;
     if (sh.overflow) {
-      failed = true;
+      overflow = true;
       break;
     }
-    if (len == 0 && sh.frontLen == 0)
+    if (len == 0 && sh.frontLen == 0 && !selfPending)
       break;
     if (p.prune && len > 1)
       sortCandidates(sh, len);
-    auto nextValid = [&](int from) {
-      while (from < len && sh.listLb[from] > sh.thrTile)
-        ++from;
-      return from;
-    };
-    int cur = nextValid(0), buf = 0;
-    if (cur < len) {
-      if (tid == 0)
-        issue(cur, buf);
-      inFlight[buf] = true;
-    }
-    while (cur < len && !failed) {
-      const int next = nextValid(cur + 1);
-      if (next < len) {
-        if (tid == 0)
-          issue(next, buf ^ 1);
-        inFlight[buf ^ 1] = true;
+    __syncthreads();
+
+    if (!consumer) {
+      // ---- producers ----
+      const int j = tid - kTile;
+      int cursor = 0;
+      bool sentinelIssued = false;
+      // Leader: the next ordinal into the ring (a column tile, or the sentinel).
+      auto issueNext = [&]() {
+        const int r = issued % kScreenStages;
+        if (!screenWait(&ss.rawEmpty[r], ((issued / kScreenStages) & 1) ^ 1, ss)) {
+          sentinelIssued = true; // nothing more goes into a slot that may be in use
+          return;
+        }
+        int entry = -1;
+        if (selfPending) {
+          entry = I;
+          selfPending = false;
+        } else {
+          const float thr = *(volatile float *)&sh.thrTile;
+          while (cursor < len && sh.listLb[cursor] > thr)
+            ++cursor;
+          if (cursor < len)
+            entry = sh.listTile[cursor++];
+        }
+        ss.rawTile[r] = entry;
+        if (entry < 0) {
+          sentinelIssued = true;
+          mbarrierArrive(&ss.rawFull[r], 1);
+        } else {
+          const int J = entry & ~kPureColumnTile;
+          int *meta = metaBase + r * L::metaInts;
+          fenceProxyAsync();
+          mbarrierArriveExpectTx(&ss.rawFull[r], tileBytes + metaBytes);
+          bulkCopyToShared(rawBase + r * L::rawFloats, p.tiled + (size_t)J * L::rawFloats,
+                           tileBytes, &ss.rawFull[r]);
+          bulkCopyToShared(meta, p.order + (size_t)J * kTile, kTile * sizeof(int),
+                           &ss.rawFull[r]);
+          if (useComp)
+            bulkCopyToShared(meta + kTile, p.component + (size_t)J * kTile, kTile * sizeof(int),
+                             &ss.rawFull[r]);
+          if (useValue)
+            bulkCopyToShared(meta + 2 * kTile, w.value + (size_t)J * kTile,
+                             kTile * sizeof(float), &ss.rawFull[r]);
+        }
+        ++issued;
+      };
+      while (true) {
+        const int s = t & 1;
+        bool ok = screenWait(&ss.tmemEmpty[s], ((t >> 1) & 1) ^ 1, ss);
+        if (leader && ok)
+          while (!sentinelIssued && issued <= t + kScreenAhead)
+            issueNext();
+        const int r = t % kScreenStages;
+        ok = screenWait(&ss.rawFull[r], (t / kScreenStages) & 1, ss) && ok;
+        const int entry = ok ? ss.rawTile[r] : -1;
+        if (entry >= 0)
+          buildColumnOperand<KC>(rawBase + r * L::rawFloats, metaBase + r * L::metaInts + kTile,
+                                 centre, scale, j, oneHot, ss, opB + (size_t)s * kTile * kPad);
+        fenceProxyAsync();
+        const bool stop = namedBarrierOr(1, kThreads - kTile, entry < 0);
+        if (leader) {
+          if (stop) {
+            ss.slotTile[s] = -1;
+            mbarrierArrive(&ss.mmaFull[s], 2);
+          } else {
+            tcgenFenceAfter();
+            const float *b = opB + (size_t)s * kTile * kPad;
+#pragma unroll
+            for (int ks = 0; ks < kPad / 8; ++ks)
+              mmaTf32(tmem + (uint32_t)(s * kTile), umma_smem_desc(opA + 64 * ks, 128, kSbo),
+                      umma_smem_desc(b + 64 * ks, 128, kSbo), idesc, ks > 0);
+            mmaCommit(&ss.mmaFull[s]);
+            lastCommit = t;
+            ss.slotTile[s] = entry;
+            mbarrierArrive(&ss.mmaFull[s], 1);
+          }
+        }
+        ++t;
+        if (stop)
+          break;
       }
-      const bool ready = mbarrierWait(&sh.bar[buf], phase[buf]);
-      phase[buf] ^= 1;
-      inFlight[buf] = false;
-      if (__syncthreads_or(!ready)) {
-        failed = true;
-        break;
+    } else {
+      // ---- consumers ----
+      float *list = lists + myRow * p.k;
+      while (true) {
+        const int s = t & 1;
+        const unsigned int cbPre = compSlot ? __ldcg(compSlot) : 0xffffffffu;
+        const bool ok = screenWait(&ss.mmaFull[s], (t >> 1) & 1, ss);
+        tcgenFenceAfter();
+        const int entry = __shfl_sync(0xffffffffu, ok ? ss.slotTile[s] : -1, 0);
+        const int r = t % kScreenStages;
+        if (entry >= 0) {
+          const int J = entry & ~kPureColumnTile;
+          const bool colPure = (entry & kPureColumnTile) != 0;
+          const float *raw = rawBase + r * L::rawFloats;
+          const int *cOrig = metaBase + r * L::metaInts;
+          const int *cComp = cOrig + kTile;
+          const float *cVal = reinterpret_cast<const float *>(cOrig + 2 * kTile);
+          const bool mask = maskPass && !oneHot && !(rowPure >= 0 && colPure);
+          const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * kTile);
+          float v[32];
+          float mn = INFINITY;
+          if (mask) {
+#pragma unroll
+            for (int chunk = 0; chunk < 4; ++chunk) {
+              tmemLoad32(taddr + chunk * 32, v);
+#pragma unroll
+              for (int q = 0; q < 8; ++q) {
+                const int4 cc = reinterpret_cast<const int4 *>(cComp)[chunk * 8 + q];
+                mn = min3(mn, cc.x != myComp ? v[4 * q] : INFINITY,
+                          cc.y != myComp ? v[4 * q + 1] : INFINITY);
+                mn = min3(mn, cc.z != myComp ? v[4 * q + 2] : INFINITY,
+                          cc.w != myComp ? v[4 * q + 3] : INFINITY);
+              }
+            }
+          } else {
+#pragma unroll
+            for (int chunk = 0; chunk < 4; ++chunk) {
+              tmemLoad32(taddr + chunk * 32, v);
+#pragma unroll
+              for (int c = 0; c < 32; c += 2)
+                mn = min3(mn, v[c], v[c + 1]);
+            }
+          }
+          float Fs = F + kScreenAbsSlack;
+          const bool want = myValid && mn <= Fs;
+          if (__any_sync(0xffffffffu, want)) {
+#pragma unroll 1
+            for (int chunk = 0; chunk < 4; ++chunk) {
+              tmemLoad32(taddr + chunk * 32, v);
+              if (!want)
+                continue;
+              unsigned candidates = 0;
+#pragma unroll
+              for (int c = 0; c < 32; ++c)
+                candidates |= (v[c] <= Fs ? 1u : 0u) << c;
+              while (candidates) {
+                const int c = __ffs(candidates) - 1;
+                candidates &= candidates - 1;
+                const int jj = chunk * 32 + c;
+                if (J * kTile + jj >= p.n)
+                  continue;
+                if (!kKnn && (useComp ? cComp[jj] : cOrig[jj]) == myComp)
+                  continue;
+                // The reference's exact FP32 distance (zero-padded features add 0).
+                typename Metric::Acc acc = m.init();
+#pragma unroll
+                for (int k = 0; k < KC; ++k)
+                  acc = m.accumulate(acc, sA[k * kTile + myRow], raw[k * kTile + jj]);
+                if (kKnn) {
+                  const float value =
+                      J * kTile + jj == myPos ? 0.0f : fmaxf(m.finalize(acc), 0.0f);
+                  insertSorted(list, p.k, value);
+                  Fs = m.filterBound(list[p.k - 1]) + kScreenAbsSlack;
+                } else {
+                  const float weight =
+                      w.weight(m.finalize(acc), myVal, useValue ? cVal[jj] : 0.0f);
+                  if (weight < INFINITY) {
+                    const unsigned long long key = packKey(weight, (uint32_t)cOrig[jj]);
+                    rowBest = key < rowBest ? key : rowBest;
+                  }
+                }
+              }
+            }
+          }
+          warpMaxThr(refresh(cbPre));
+          ++computed;
+        }
+        tcgenFenceBefore();
+        const bool stop = namedBarrierOr(2, kTile, entry < 0);
+        if (tid == 0) {
+          mbarrierArrive(&ss.tmemEmpty[s], 1);
+          mbarrierArrive(&ss.rawEmpty[r], 1);
+          if (!stop)
+            *(volatile float *)&sh.thrTile =
+                fmaxf(fmaxf(ss.warpThr[0], ss.warpThr[1]), fmaxf(ss.warpThr[2], ss.warpThr[3]));
+        }
+        ++t;
+        if (stop)
+          break;
       }
-      if (sh.listLb[cur] <= sh.thrTile)
-        processTile(sh.listTile[cur] & ~kPureColumnTile, sB[buf], meta[buf],
-                    (sh.listTile[cur] & kPureColumnTile) != 0);
-      else
-        __syncthreads();
-      cur = next;
-      buf ^= 1;
     }
     __syncthreads();
+    // The leader issued the row tile itself first in the first batch; every
+    // thread forgets it here so that the loop's exit stays uniform.
+    selfPending = false;
+    if (ss.failed)
+      break;
     if (sh.frontLen == 0)
       break;
   }
 
-  for (int b = 0; b < 2; ++b)
-    if (inFlight[b])
-      mbarrierWait(&sh.bar[b], phase[b]);
-  if (tid < kTile) {
-    const int pos = firstRow + tid;
-    if (pos < p.n) {
-      if (kKnn)
-        p.core[pos] = lists[tid * p.k + p.k - 1];
-      else
-        p.nearest[pos] = sh.rowBest[tid];
-    }
+  // Nothing may land in shared or tensor memory after the block leaves: on a
+  // failure the leader waits (bounded) for its copies and its last MMAs.
+  if (leader && ss.failed) {
+    for (int o = t; o < issued; ++o)
+      mbarrierWait(&ss.rawFull[o % kScreenStages], (o / kScreenStages) & 1);
+    if (lastCommit >= 0)
+      mbarrierWait(&ss.mmaFull[lastCommit & 1], (lastCommit >> 1) & 1);
   }
-  // Tensor memory goes back before the block leaves, on every path.
+  if (myValid) {
+    if (kKnn)
+      p.core[myPos] = lists[myRow * p.k + p.k - 1];
+    else
+      p.nearest[myPos] = rowBest;
+  }
   tcgenFenceBefore();
   __syncthreads();
   if (warp == 0) {
     tcgenFenceAfter();
-    tmemDealloc(tmem, kTile);
+    tmemDealloc(tmem, 256);
   }
   if (tid == 0) {
     if (p.tilesComputed)
       atomicAdd(p.tilesComputed, computed);
-    if (failed && p.error)
-      atomicCAS(p.error, 0, sh.overflow ? (int)kErrorTooLarge : (int)kErrorTimeout);
+    if ((ss.failed || overflow) && p.error)
+      atomicCAS(p.error, 0, overflow ? (int)kErrorTooLarge : (int)kErrorTimeout);
   }
 }
 
@@ -391,39 +583,53 @@ template <> struct ScreenSupport<SqEuclideanMetric> {
   static constexpr bool value = true;
 };
 
-// Dynamic shared memory of a screened pass block (k = 0: nearest pass).
+// Shared memory a block may use on sm_100 (227 KiB); a screened block keeps
+// at least kScreenMinShared so that at most two share an SM (their tensor
+// memory, 256 columns each, then always fits).
+constexpr size_t kMaxBlockShared = 227 * 1024;
+constexpr size_t kScreenMinShared = 80 * 1024;
+
 inline size_t screenDynamicBytes(int d, int k) {
-  const int kc = chunkWidthFor(d);
-  return (size_t)3 * kc * kTile * sizeof(float) + 6 * kTile * sizeof(int) +
-         (size_t)2 * kTile * screenK(d) * sizeof(float) + (size_t)(3 * d + kTile * k) * sizeof(float);
+  size_t bytes;
+  switch (chunkWidthFor(d)) {
+  case 4:
+    bytes = ScreenLayout<4>::bytes(k);
+    break;
+  case 8:
+    bytes = ScreenLayout<8>::bytes(k);
+    break;
+  case 16:
+    bytes = ScreenLayout<16>::bytes(k);
+    break;
+  default:
+    bytes = ScreenLayout<32>::bytes(k);
+    break;
+  }
+  const size_t fixed = sizeof(PassState) + sizeof(ScreenSync);
+  return bytes + fixed < kScreenMinShared ? kScreenMinShared - fixed : bytes;
 }
 
-// Shared memory a block may use on sm_100 (227 KiB).
-constexpr size_t kMaxBlockShared = 227 * 1024;
-
-// Whether a pass over d features (k-NN rank k, 0 for a nearest pass) runs
+// Whether a pass over d features (k-NN rank k, 0 for a nearest pass) can run
 // screened: the metric has a screened form, the features fit one chunk of at
 // most 32, the block's shared memory fits, and screening is not switched off.
+// Callers also check the data's extent (SpatialIndex::screenRangeOk).
 template <class Metric> inline bool useScreen(int d, int k) {
   return ScreenSupport<Metric>::value && currentScreenMode() != 2 &&
          chunkWidthFor(d) * numChunksFor(d) <= 32 &&
-         screenDynamicBytes(d, k) + sizeof(PassState) + 64 <= kMaxBlockShared;
+         screenDynamicBytes(d, k) + sizeof(PassState) + sizeof(ScreenSync) <= kMaxBlockShared;
 }
 
-// Launches the screened pass; returns a negative code when the metric or the
-// dimension has no screened form (callers then use launchPass).
+// Launches the screened pass; a negative code when the metric or the
+// dimension has no screened form (callers check useScreen first).
 template <class Metric, class Weight, bool kKnn>
 int launchScreen(const PassParams &p, const Metric &m, const Weight &w, int kc,
                  cudaStream_t stream) {
   if constexpr (!ScreenSupport<Metric>::value) {
     return kErrorInvalidAlgorithm;
   } else {
-    if (p.numChunks != 1)
+    if (p.numChunks != 1 || kc != chunkWidthFor(p.d))
       return kErrorInvalidAlgorithm;
-    const int kPad = screenK(p.d);
-    const float margin = screenMargin(p.d);
-    if (kc != chunkWidthFor(p.d))
-      return kErrorInvalidAlgorithm;
+    const float margin = screenMargin(p.d, kc);
     const size_t dynBytes = screenDynamicBytes(p.d, kKnn ? p.k : 0);
     auto misaligned = [](const void *ptr) { return ((uintptr_t)ptr & 15) != 0; };
     if (misaligned(p.tiled) || misaligned(p.order) || misaligned(p.component) ||
@@ -434,7 +640,7 @@ int launchScreen(const PassParams &p, const Metric &m, const Weight &w, int kc,
           cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dynBytes);
       if (e != cudaSuccess)
         return (int)e;
-      kernel<<<p.numTiles, kThreads, dynBytes, stream>>>(p, m, w, margin, kPad);
+      kernel<<<p.numTiles, kThreads, dynBytes, stream>>>(p, m, w, margin);
       noteLaunch();
       return (int)cudaGetLastError();
     };

@@ -3,6 +3,7 @@
 #include "spatial.cuh"
 
 #include <algorithm>
+#include <vector>
 #include <cub/device/device_radix_sort.cuh>
 
 namespace cuhc {
@@ -385,6 +386,20 @@ int SpatialIndex::updateMinValues(const float *values) {
         lb, le, nodeLeft.get(), nodeRight.get(), nodeMinValue.get(), nullptr); noteLaunch();
   }
   return (int)cudaGetLastError();
+}
+
+bool SpatialIndex::extentsWithin(float limit) {
+  std::vector<float> low(d), high(d);
+  if (cudaMemcpyAsync(low.data(), nodeLow.get(), d * sizeof(float), cudaMemcpyDeviceToHost,
+                      stream) != cudaSuccess ||
+      cudaMemcpyAsync(high.data(), nodeHigh.get(), d * sizeof(float), cudaMemcpyDeviceToHost,
+                      stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return false;
+  for (int f = 0; f < d; ++f)
+    if (!(high[f] - low[f] <= limit)) // NaN fails too
+      return false;
+  return true;
 }
 
 int SpatialIndex::updatePurity(const int *component) {

@@ -58,6 +58,10 @@ struct SpatialIndex {
   int updateMinValues(const float *valuesByPosition);
   // Per-node purity of component[position] (null: every node impure).
   int updatePurity(const int *componentByPosition);
+  // Whether every coordinate's extent over all points (the root box) is
+  // finite and at most `limit`. Copies the root box to the host and waits
+  // for the index stream.
+  bool extentsWithin(float limit);
 };
 
 } // namespace cuhc
