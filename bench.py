@@ -281,8 +281,10 @@ def main():
     # Kernel-level figures: the pass kernels timed on their own stream.
     _lib.set_timing(True)
     _lib.kernel_timing()
+    _lib.screen_counters()
     timed(device_step, 1)
     kt = _lib.kernel_timing()
+    sc = _lib.screen_counters()
     _lib.set_timing(False)
 
     # The same step with tensor-core screening switched off (plain FP32 passes).
@@ -359,6 +361,9 @@ def main():
                            "note": "same step with tensor-core screening off"},
             "passes": {**{k: {"ms": round(v[0], 2), "launches": v[1], "tiles": v[2]}
                           for k, v in kt.items()},
+                       "screen": {**sc, "rechecks_per_pair": round(
+                           sc["rechecks"] / max(1, 16384 * sum(
+                               v[2] for k, v in kt.items() if k.startswith("screen"))), 6)},
                        "tiles_per_step": int((stats1[0] - stats0[0]) / max(args.steps, 1)),
                        "rounds_per_step": (stats1[3] - stats0[3]) / max(args.steps, 1)},
             "clocks": clocks.summary(),

@@ -54,6 +54,8 @@ lib.cuhc_pass_stats.argtypes = [_u64, _int]
 lib.cuhc_hdbscan_labels.restype = _int
 lib.cuhc_hdbscan_labels.argtypes = [_f64, ctypes.c_int64, ctypes.c_int64, _int, _int,
                                     ctypes.c_double, ctypes.c_int64, _i64, _f64]
+lib.cuhc_screen_counters.restype = _int
+lib.cuhc_screen_counters.argtypes = [ctypes.POINTER(ctypes.c_uint64), _int]
 lib.cuhc_set_screen.restype = _int
 lib.cuhc_set_screen.argtypes = [_int]
 lib.cuhc_launch_count.restype = ctypes.c_uint64
@@ -100,6 +102,19 @@ def set_screen(mode):
     and sqeuclidean up to 32 features), "on" or "off". Results are identical
     in every mode; only the time changes."""
     check(lib.cuhc_set_screen(SCREEN_MODES[mode]))
+
+
+SCREEN_COUNTERS = ("rechecks", "slow_rows", "indicator_tiles", "masked_tiles")
+
+
+def screen_counters():
+    """Screened-pass counters since the last call (counted while timing is
+    on): exact rechecks, row visits that took the exact path, tiles whose
+    components were excluded by indicator slots, tiles masked in the
+    epilogue."""
+    out = (ctypes.c_uint64 * 4)()
+    check(lib.cuhc_screen_counters(out, 4))
+    return dict(zip(SCREEN_COUNTERS, (int(x) for x in out)))
 
 
 def prune_stats():

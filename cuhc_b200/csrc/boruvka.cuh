@@ -203,6 +203,7 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
   p.compBest = compBest.get();
   p.tilesComputed = tiles.get();
   p.error = error.get();
+  p.screenStats = screenCounters();
 
   const bool screened = useScreen<Metric>(index.d, 0) && index.extentsWithin(kScreenMaxExtent);
   int numComponents = n, totalEdges = 0, rounds = 0;
@@ -332,6 +333,7 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
   p.k = k;
   p.tilesComputed = tiles.get();
   p.error = error.get();
+  p.screenStats = screenCounters();
   {
     const bool screened =
         useScreen<Metric>(index.d, k) && index.extentsWithin(kScreenMaxExtent);

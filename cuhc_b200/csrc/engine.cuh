@@ -156,6 +156,7 @@ struct PassParams {
   int k;                          // knn-mode rank
   unsigned long long *tilesComputed;
   int *error;
+  unsigned long long *screenStats; // ScreenCounter sums (null: not counted)
 };
 
 // Lower bound of every distance between the row tile box (shared memory)

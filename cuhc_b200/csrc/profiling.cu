@@ -12,8 +12,19 @@ double gMs[kNumTimers] = {};
 unsigned long long gCount[kNumTimers] = {}, gTiles[kNumTimers] = {};
 } // namespace
 
+__device__ unsigned long long gScreenCounterArray[kNumScreenCounters];
+
 void noteLaunch(int count) { gLaunches.fetch_add((unsigned long long)count); }
 bool timingEnabled() { return gTiming.load() != 0; }
+
+unsigned long long *screenCounters() {
+  if (!timingEnabled())
+    return nullptr;
+  void *ptr = nullptr;
+  if (cudaGetSymbolAddress(&ptr, gScreenCounterArray) != cudaSuccess)
+    return nullptr;
+  return static_cast<unsigned long long *>(ptr);
+}
 
 PassTimer::PassTimer(int k, cudaStream_t s) : kind(k), stream(s) {
   if (!timingEnabled())
@@ -54,7 +65,8 @@ int cuhc_set_timing(int on) {
   return 0;
 }
 
-// Per pass kind (0 k-NN pass, 1 nearest pass, 2 screened pass): summed
+// Per pass kind (0 k-NN pass, 1 nearest pass, 2 screened nearest pass,
+// 3 screened k-NN pass): summed
 // device milliseconds, launches and tiles computed since the last call;
 // resets them.
 int cuhc_kernel_timing(double *ms, unsigned long long *launches, unsigned long long *tiles,
@@ -68,6 +80,21 @@ int cuhc_kernel_timing(double *ms, unsigned long long *launches, unsigned long l
     cuhc::gCount[i] = cuhc::gTiles[i] = 0;
   }
   return 0;
+}
+
+// Screened-pass counters of the current device since the last call (first
+// `count` of: exact rechecks, exact-path row visits, indicator tiles, masked
+// tiles); resets them. Counted only while timing is on.
+int cuhc_screen_counters(unsigned long long *out, int count) {
+  unsigned long long host[cuhc::kNumScreenCounters] = {};
+  cudaError_t e = cudaMemcpyFromSymbol(host, cuhc::gScreenCounterArray, sizeof(host));
+  if (e == cudaSuccess) {
+    const unsigned long long zero[cuhc::kNumScreenCounters] = {};
+    e = cudaMemcpyToSymbol(cuhc::gScreenCounterArray, zero, sizeof(zero));
+  }
+  for (int i = 0; i < count && i < cuhc::kNumScreenCounters; ++i)
+    out[i] = host[i];
+  return (int)e;
 }
 
 } // extern "C"

@@ -18,6 +18,15 @@ enum TimerKind : int { kTimerKnnPass = 0, kTimerNearestPass = 1, kTimerScreenPas
 void noteLaunch(int count = 1);
 bool timingEnabled();
 
+// Screened-pass counters (device memory of the current device), summed by
+// the screened kernels while timing is on: exact rechecks, row visits that
+// took the exact path, tiles whose components were excluded by indicator
+// slots, tiles masked by component in the epilogue.
+enum ScreenCounter : int { kScreenRechecks = 0, kScreenSlowRows = 1, kScreenIndicatorTiles = 2,
+                           kScreenMaskedTiles = 3, kNumScreenCounters = 4 };
+// Null when timing is off (the kernels then count nothing).
+unsigned long long *screenCounters();
+
 // RAII bracket around one pass launch; records only when timing is on.
 struct PassTimer {
   int kind;

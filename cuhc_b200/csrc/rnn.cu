@@ -281,6 +281,7 @@ int rnnWard(const float *devPoints, int n, int d, const RnnOptions &options, dou
     p.compBest = nullptr;
     p.tilesComputed = tiles.get();
     p.error = error.get();
+  p.screenStats = screenCounters();
     WardWeight w;
     w.value = sizeF[cur].get();
     {

@@ -28,19 +28,22 @@
 // epilogue masks by component.
 //
 // Pipeline, warp-specialised, one row tile per block:
-//   producer warps 4-7 (column j = thread - 128): build the column operand of
-//     each staged column tile; thread 128 also issues the bulk copies (raw
-//     coordinates + metadata, a ring of four, two ahead) and the MMAs;
+//   control warp 7 (one thread): issues the bulk copies of column tiles (raw
+//     coordinates + metadata, a ring of five, two ahead) and the MMAs;
+//   builder warps 4-6: build the column operand of each staged tile (warp 4
+//     two columns per thread) as soon as the MMA that last read its buffer is
+//     done;
 //   consumer warps 0-3 (row i = thread = tensor-memory lane): read the
 //     accumulator, take the row minimum, recheck rows with a pair at or below
-//     their filter, refresh the row threshold.
-// Tensor memory holds two 128 x 128 FP32 accumulators, so the producers
-// build and multiply tile t + 1 while the consumers read tile t. mbarriers
-// link the stages: rawFull (copy landed), mmaFull (MMA done + slot info),
-// tmemEmpty / rawEmpty (consumers done). Candidate collection and ordering
-// are those of passes.cuh, one batch at a time; a sentinel ends each batch.
-// Every wait is bounded; one that runs out stops both groups at the same
-// ordinal and the pass returns kErrorTimeout.
+//     their filter, refresh the row threshold when it may have changed.
+// Tensor memory holds two 128 x 128 FP32 accumulators, so the MMAs of tile
+// t + 1 run while the consumers read tile t. mbarriers link the stages:
+// rawFull (copy landed), opBReady (operand built), mmaFull (MMA done + slot
+// info), tmemEmpty (every consumer warp done with the accumulator, and so
+// with the ring slot two ordinals back). Candidate collection and ordering
+// are those of passes.cuh, one batch at a time; a sentinel ordinal ends each
+// batch. Every wait is bounded; one that runs out marks the block failed,
+// every later wait gives up at once, and the pass returns kErrorTimeout.
 #pragma once
 
 #include <climits>
@@ -55,9 +58,12 @@ namespace cuhc {
 // terms and at least 4 component slots, a multiple of the MMA's K step (8).
 __host__ __device__ constexpr int screenKPad(int kc) { return (kc + 8 + 7) / 8 * 8; }
 __host__ __device__ constexpr int screenSlots(int kc) { return screenKPad(kc) - kc - 4; }
-constexpr int kScreenStages = 4; // column tiles staged in shared memory
+constexpr int kScreenStages = 5; // column tiles staged in shared memory
 constexpr int kScreenAhead = 2;  // copies issued ahead of the tile being built
 constexpr int kScreenMaxSlots = 8;
+constexpr int kBuilderWarps = 3; // warps 4..6 build column operands
+constexpr int kBuilderThreads = 32 * kBuilderWarps;
+constexpr int kControlWarp = 7;  // issues the bulk copies and the MMAs
 constexpr float kIndicator = 0x1p90f;
 constexpr float kScreenAbsSlack = 0x1p-70f;
 constexpr float kScreenMaxExtent = 0x1p40f;
@@ -89,8 +95,8 @@ template <int KC> struct ScreenLayout {
 };
 
 struct ScreenSync {
-  uint64_t rawFull[kScreenStages], rawEmpty[kScreenStages];
-  uint64_t mmaFull[2], tmemEmpty[2];
+  uint64_t rawFull[kScreenStages];
+  uint64_t mmaFull[2], tmemEmpty[2], opBReady[2];
   int rawTile[kScreenStages]; // column tile (| kPureColumnTile) per ring slot, -1 ends the batch
   int slotTile[2];            // the same, per accumulator
   float warpThr[4];
@@ -199,7 +205,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool consumer = tid < kTile;
-  const bool leader = tid == kTile;
+  const bool control = tid == kControlWarp * 32;
   const int I = blockIdx.x;
   const int firstRow = I * kTile;
   const int leaf = p.leafOfTile[I];
@@ -239,13 +245,15 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (consumer && wantOneHot)
     rowComps[myRow] = myValid ? myComp : -1;
   if (tid == 0) {
-    for (int s = 0; s < kScreenStages; ++s) {
+    // Arrival counts: rawFull takes the control's expect-tx (or sentinel)
+    // arrival, mmaFull the MMA commit + the control's release of slotTile,
+    // tmemEmpty one per consumer warp, opBReady one per builder warp.
+    for (int s = 0; s < kScreenStages; ++s)
       mbarrierInit(&ss.rawFull[s], 1);
-      mbarrierInit(&ss.rawEmpty[s], 1);
-    }
     for (int s = 0; s < 2; ++s) {
-      mbarrierInit(&ss.mmaFull[s], 2); // the MMA commit + the issuer's release of slotTile
-      mbarrierInit(&ss.tmemEmpty[s], 1);
+      mbarrierInit(&ss.mmaFull[s], 2);
+      mbarrierInit(&ss.tmemEmpty[s], 4);
+      mbarrierInit(&ss.opBReady[s], kBuilderWarps);
     }
     fenceBarrierInit();
     ss.failed = 0;
@@ -329,11 +337,13 @@ __global__ void __launch_bounds__(kThreads, 2)
   const uint32_t metaBytes = (uint32_t)(kTile * sizeof(int)) * (1 + useComp + useValue);
   const uint32_t tileBytes = (uint32_t)(L::rawFloats * sizeof(float));
   int t = 0;      // ordinal of tiles and sentinels through the rings (all threads agree)
-  int issued = 0; // leader: ordinals issued
+  int issued = 0; // control: ordinals issued
   int lastCommit = -1;
   unsigned long long computed = 0;
   bool selfPending = kKnn || rowPure < 0;
   bool overflow = false;
+  bool dirty = false;                          // consumer: row filter may have tightened
+  unsigned long long rechecks = 0, slowRows = 0; // consumer counters
 
   while (true) {
     if (warp == 0)
@@ -350,70 +360,64 @@ __global__ void __launch_bounds__(kThreads, 2)
       sortCandidates(sh, len);
     __syncthreads();
 
-    if (!consumer) {
-      // ---- producers ----
-      const int j = tid - kTile;
-      int cursor = 0;
-      bool sentinelIssued = false;
-      // Leader: the next ordinal into the ring (a column tile, or the sentinel).
-      auto issueNext = [&]() {
-        const int r = issued % kScreenStages;
-        if (!screenWait(&ss.rawEmpty[r], ((issued / kScreenStages) & 1) ^ 1, ss)) {
-          sentinelIssued = true; // nothing more goes into a slot that may be in use
-          return;
-        }
-        int entry = -1;
-        if (selfPending) {
-          entry = I;
-          selfPending = false;
-        } else {
-          const float thr = *(volatile float *)&sh.thrTile;
-          while (cursor < len && sh.listLb[cursor] > thr)
-            ++cursor;
-          if (cursor < len)
-            entry = sh.listTile[cursor++];
-        }
-        ss.rawTile[r] = entry;
-        if (entry < 0) {
-          sentinelIssued = true;
-          mbarrierArrive(&ss.rawFull[r], 1);
-        } else {
-          const int J = entry & ~kPureColumnTile;
-          int *meta = metaBase + r * L::metaInts;
-          fenceProxyAsync();
-          mbarrierArriveExpectTx(&ss.rawFull[r], tileBytes + metaBytes);
-          bulkCopyToShared(rawBase + r * L::rawFloats, p.tiled + (size_t)J * L::rawFloats,
-                           tileBytes, &ss.rawFull[r]);
-          bulkCopyToShared(meta, p.order + (size_t)J * kTile, kTile * sizeof(int),
-                           &ss.rawFull[r]);
-          if (useComp)
-            bulkCopyToShared(meta + kTile, p.component + (size_t)J * kTile, kTile * sizeof(int),
-                             &ss.rawFull[r]);
-          if (useValue)
-            bulkCopyToShared(meta + 2 * kTile, w.value + (size_t)J * kTile,
-                             kTile * sizeof(float), &ss.rawFull[r]);
-        }
-        ++issued;
-      };
-      while (true) {
-        const int s = t & 1;
-        bool ok = screenWait(&ss.tmemEmpty[s], ((t >> 1) & 1) ^ 1, ss);
-        if (leader && ok)
-          while (!sentinelIssued && issued <= t + kScreenAhead)
-            issueNext();
-        const int r = t % kScreenStages;
-        ok = screenWait(&ss.rawFull[r], (t / kScreenStages) & 1, ss) && ok;
-        const int entry = ok ? ss.rawTile[r] : -1;
-        if (entry >= 0)
-          buildColumnOperand<KC>(rawBase + r * L::rawFloats, metaBase + r * L::metaInts + kTile,
-                                 centre, scale, j, oneHot, ss, opB + (size_t)s * kTile * kPad);
-        fenceProxyAsync();
-        const bool stop = namedBarrierOr(1, kThreads - kTile, entry < 0);
-        if (leader) {
-          if (stop) {
-            ss.slotTile[s] = -1;
-            mbarrierArrive(&ss.mmaFull[s], 2);
+    if (warp == kControlWarp) {
+      // ---- control: bulk copies and MMAs (lane 0) ----
+      if (lane == 0) {
+        int cursor = 0;
+        bool sentinelIssued = false;
+        // Issues ordinal `issued` into its ring slot: a column tile, or the
+        // batch's sentinel. The slot's previous ordinal (issued - stages) is
+        // done with: at a batch start every ordinal is, and later the caller
+        // has seen every consumer warp release ordinal issued - kScreenAhead
+        // - 2, which each of them does after finishing issued - stages.
+        auto issueNext = [&]() {
+          const int r = issued % kScreenStages;
+          int entry = -1;
+          if (selfPending) {
+            entry = I;
+            selfPending = false;
           } else {
+            const float thr = *(volatile float *)&sh.thrTile;
+            while (cursor < len && sh.listLb[cursor] > thr)
+              ++cursor;
+            if (cursor < len)
+              entry = sh.listTile[cursor++];
+          }
+          ss.rawTile[r] = entry;
+          if (entry < 0) {
+            sentinelIssued = true;
+            mbarrierArrive(&ss.rawFull[r], 1);
+          } else {
+            const int J = entry & ~kPureColumnTile;
+            int *meta = metaBase + r * L::metaInts;
+            mbarrierArriveExpectTx(&ss.rawFull[r], tileBytes + metaBytes);
+            bulkCopyToShared(rawBase + r * L::rawFloats, p.tiled + (size_t)J * L::rawFloats,
+                             tileBytes, &ss.rawFull[r]);
+            bulkCopyToShared(meta, p.order + (size_t)J * kTile, kTile * sizeof(int),
+                             &ss.rawFull[r]);
+            if (useComp)
+              bulkCopyToShared(meta + kTile, p.component + (size_t)J * kTile,
+                               kTile * sizeof(int), &ss.rawFull[r]);
+            if (useValue)
+              bulkCopyToShared(meta + 2 * kTile, w.value + (size_t)J * kTile,
+                               kTile * sizeof(float), &ss.rawFull[r]);
+          }
+          ++issued;
+        };
+        while (!sentinelIssued && issued <= t + kScreenAhead)
+          issueNext();
+        while (true) {
+          const int s = t & 1;
+          // Every consumer warp released ordinal t - 2: accumulator s is
+          // free, and so is the ring slot of ordinal t + kScreenAhead.
+          bool ok = screenWait(&ss.tmemEmpty[s], ((t >> 1) & 1) ^ 1, ss);
+          if (ok)
+            while (!sentinelIssued && issued <= t + kScreenAhead)
+              issueNext();
+          const int entry = ss.rawTile[t % kScreenStages];
+          // The builders finished the column operand of ordinal t.
+          ok = ok && entry >= 0 && screenWait(&ss.opBReady[s], (t >> 1) & 1, ss);
+          if (ok) {
             tcgenFenceAfter();
             const float *b = opB + (size_t)s * kTile * kPad;
 #pragma unroll
@@ -424,22 +428,53 @@ __global__ void __launch_bounds__(kThreads, 2)
             lastCommit = t;
             ss.slotTile[s] = entry;
             mbarrierArrive(&ss.mmaFull[s], 1);
+          } else {
+            ss.slotTile[s] = -1; // the batch's end (or a failed wait) goes on to the consumers
+            mbarrierArrive(&ss.mmaFull[s], 2);
           }
+          ++t;
+          if (!ok)
+            break;
         }
+      }
+      t = __shfl_sync(0xffffffffu, t, 0);
+    } else if (!consumer) {
+      // ---- builders: warps 4..6, column j and (warp 4) column j + 96 ----
+      const int j = tid - kTile;
+      while (true) {
+        const int s = t & 1;
+        // The operand buffer of slot s is free once the MMA of ordinal t - 2
+        // has completed (the consumers may still be reading its result).
+        bool ok = screenWait(&ss.mmaFull[s], ((t >> 1) & 1) ^ 1, ss);
+        const int r = t % kScreenStages;
+        ok = screenWait(&ss.rawFull[r], (t / kScreenStages) & 1, ss) && ok;
+        const int entry = __shfl_sync(0xffffffffu, ok ? ss.rawTile[r] : -1, 0);
+        if (entry >= 0) {
+          const float *raw = rawBase + r * L::rawFloats;
+          const int *comp = metaBase + r * L::metaInts + kTile;
+          float *b = opB + (size_t)s * kTile * kPad;
+          buildColumnOperand<KC>(raw, comp, centre, scale, j, oneHot, ss, b);
+          if (j < kTile - kBuilderThreads)
+            buildColumnOperand<KC>(raw, comp, centre, scale, j + kBuilderThreads, oneHot, ss, b);
+        }
+        fenceProxyAsync();
+        __syncwarp();
+        if (lane == 0)
+          mbarrierArrive(&ss.opBReady[s], 1);
         ++t;
-        if (stop)
+        if (entry < 0)
           break;
       }
     } else {
-      // ---- consumers ----
+      // ---- consumers: warps 0..3, row myRow = tensor-memory lane ----
       float *list = lists + myRow * p.k;
       while (true) {
         const int s = t & 1;
-        const unsigned int cbPre = compSlot ? __ldcg(compSlot) : 0xffffffffu;
         const bool ok = screenWait(&ss.mmaFull[s], (t >> 1) & 1, ss);
         tcgenFenceAfter();
         const int entry = __shfl_sync(0xffffffffu, ok ? ss.slotTile[s] : -1, 0);
         const int r = t % kScreenStages;
+        bool thrChanged = false;
         if (entry >= 0) {
           const int J = entry & ~kPureColumnTile;
           const bool colPure = (entry & kPureColumnTile) != 0;
@@ -449,33 +484,52 @@ __global__ void __launch_bounds__(kThreads, 2)
           const float *cVal = reinterpret_cast<const float *>(cOrig + 2 * kTile);
           const bool mask = maskPass && !oneHot && !(rowPure >= 0 && colPure);
           const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * kTile);
-          float v[32];
-          float mn = INFINITY;
-          if (mask) {
+          // Row minimum of D' (own component excluded when masking): two
+          // 32-column loads in flight per wait, eight independent chains.
+          float mn;
+          {
+            float part[8];
 #pragma unroll
-            for (int chunk = 0; chunk < 4; ++chunk) {
-              tmemLoad32(taddr + chunk * 32, v);
+            for (int q = 0; q < 8; ++q)
+              part[q] = INFINITY;
 #pragma unroll
-              for (int q = 0; q < 8; ++q) {
-                const int4 cc = reinterpret_cast<const int4 *>(cComp)[chunk * 8 + q];
-                mn = min3(mn, cc.x != myComp ? v[4 * q] : INFINITY,
-                          cc.y != myComp ? v[4 * q + 1] : INFINITY);
-                mn = min3(mn, cc.z != myComp ? v[4 * q + 2] : INFINITY,
-                          cc.w != myComp ? v[4 * q + 3] : INFINITY);
+            for (int half = 0; half < 2; ++half) {
+              uint32_t a[32], b[32];
+              tmemLoad32Async(taddr + half * 64, a);
+              tmemLoad32Async(taddr + half * 64 + 32, b);
+              tmemWaitLoads(a);
+              tmemHold(b);
+              if (mask) {
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                  const uint32_t *src = q < 8 ? a : b;
+                  const int c = (q & 7) * 4;
+                  const int4 cc = reinterpret_cast<const int4 *>(cComp)[half * 16 + q];
+                  part[q & 7] = min3(part[q & 7],
+                                     cc.x != myComp ? __uint_as_float(src[c]) : INFINITY,
+                                     cc.y != myComp ? __uint_as_float(src[c + 1]) : INFINITY);
+                  part[q & 7] = min3(part[q & 7],
+                                     cc.z != myComp ? __uint_as_float(src[c + 2]) : INFINITY,
+                                     cc.w != myComp ? __uint_as_float(src[c + 3]) : INFINITY);
+                }
+              } else {
+#pragma unroll
+                for (int c = 0; c < 32; c += 2) {
+                  part[(c >> 1) & 7] = min3(part[(c >> 1) & 7], __uint_as_float(a[c]),
+                                            __uint_as_float(a[c + 1]));
+                  part[(c >> 1) & 7] = min3(part[(c >> 1) & 7], __uint_as_float(b[c]),
+                                            __uint_as_float(b[c + 1]));
+                }
               }
             }
-          } else {
-#pragma unroll
-            for (int chunk = 0; chunk < 4; ++chunk) {
-              tmemLoad32(taddr + chunk * 32, v);
-#pragma unroll
-              for (int c = 0; c < 32; c += 2)
-                mn = min3(mn, v[c], v[c + 1]);
-            }
+            mn = fminf(fminf(min3(part[0], part[1], part[2]), min3(part[3], part[4], part[5])),
+                       fminf(part[6], part[7]));
           }
           float Fs = F + kScreenAbsSlack;
           const bool want = myValid && mn <= Fs;
           if (__any_sync(0xffffffffu, want)) {
+            slowRows += want;
+            float v[32];
 #pragma unroll 1
             for (int chunk = 0; chunk < 4; ++chunk) {
               tmemLoad32(taddr + chunk * 32, v);
@@ -498,41 +552,55 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
                 for (int k = 0; k < KC; ++k)
                   acc = m.accumulate(acc, sA[k * kTile + myRow], raw[k * kTile + jj]);
+                ++rechecks;
                 if (kKnn) {
                   const float value =
                       J * kTile + jj == myPos ? 0.0f : fmaxf(m.finalize(acc), 0.0f);
-                  insertSorted(list, p.k, value);
-                  Fs = m.filterBound(list[p.k - 1]) + kScreenAbsSlack;
+                  if (value < list[p.k - 1]) {
+                    insertSorted(list, p.k, value);
+                    Fs = m.filterBound(list[p.k - 1]) + kScreenAbsSlack;
+                    dirty = true;
+                  }
                 } else {
                   const float weight =
                       w.weight(m.finalize(acc), myVal, useValue ? cVal[jj] : 0.0f);
                   if (weight < INFINITY) {
                     const unsigned long long key = packKey(weight, (uint32_t)cOrig[jj]);
-                    rowBest = key < rowBest ? key : rowBest;
+                    if (key < rowBest) {
+                      rowBest = key;
+                      dirty = true;
+                    }
                   }
                 }
               }
             }
           }
-          warpMaxThr(refresh(cbPre));
+          // The row's filter changes only through its own exact path or the
+          // component's best (found by other blocks): refresh then, and every
+          // eighth tile for the latter.
+          if (__any_sync(0xffffffffu, dirty) || (computed & 7) == 7) {
+            warpMaxThr(refresh(compSlot ? __ldcg(compSlot) : 0xffffffffu));
+            dirty = false;
+            thrChanged = true;
+          }
           ++computed;
         }
         tcgenFenceBefore();
-        const bool stop = namedBarrierOr(2, kTile, entry < 0);
-        if (tid == 0) {
+        __syncwarp();
+        if (lane == 0) {
+          // This warp is done with accumulator s and ring slot r.
           mbarrierArrive(&ss.tmemEmpty[s], 1);
-          mbarrierArrive(&ss.rawEmpty[r], 1);
-          if (!stop)
-            *(volatile float *)&sh.thrTile =
-                fmaxf(fmaxf(ss.warpThr[0], ss.warpThr[1]), fmaxf(ss.warpThr[2], ss.warpThr[3]));
+          if (thrChanged)
+            *(volatile float *)&sh.thrTile = fmaxf(fmaxf(ss.warpThr[0], ss.warpThr[1]),
+                                                   fmaxf(ss.warpThr[2], ss.warpThr[3]));
         }
         ++t;
-        if (stop)
+        if (entry < 0)
           break;
       }
     }
     __syncthreads();
-    // The leader issued the row tile itself first in the first batch; every
+    // The control issued the row tile itself first in the first batch; every
     // thread forgets it here so that the loop's exit stays uniform.
     selfPending = false;
     if (ss.failed)
@@ -542,8 +610,8 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
 
   // Nothing may land in shared or tensor memory after the block leaves: on a
-  // failure the leader waits (bounded) for its copies and its last MMAs.
-  if (leader && ss.failed) {
+  // failure the control waits (bounded) for its copies and its last MMAs.
+  if (control && ss.failed) {
     for (int o = t; o < issued; ++o)
       mbarrierWait(&ss.rawFull[o % kScreenStages], (o / kScreenStages) & 1);
     if (lastCommit >= 0)
@@ -555,6 +623,16 @@ __global__ void __launch_bounds__(kThreads, 2)
     else
       p.nearest[myPos] = rowBest;
   }
+  if (consumer && p.screenStats) {
+    for (int off = 16; off > 0; off /= 2) {
+      rechecks += __shfl_xor_sync(0xffffffffu, rechecks, off);
+      slowRows += __shfl_xor_sync(0xffffffffu, slowRows, off);
+    }
+    if (lane == 0) {
+      atomicAdd(p.screenStats + kScreenRechecks, rechecks);
+      atomicAdd(p.screenStats + kScreenSlowRows, slowRows);
+    }
+  }
   tcgenFenceBefore();
   __syncthreads();
   if (warp == 0) {
@@ -564,6 +642,8 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (tid == 0) {
     if (p.tilesComputed)
       atomicAdd(p.tilesComputed, computed);
+    if (p.screenStats && maskPass)
+      atomicAdd(p.screenStats + (oneHot ? kScreenIndicatorTiles : kScreenMaskedTiles), computed);
     if ((ss.failed || overflow) && p.error)
       atomicCAS(p.error, 0, overflow ? (int)kErrorTooLarge : (int)kErrorTimeout);
   }
