@@ -97,6 +97,15 @@ int cuhc_hdbscan_tree_device(const float *devicePoints, int numPoints, int numFe
                              int metricId, float metricParam, int minSamples, float alpha,
                              int coreMethod, double *tree, float *core);
 
+/* HDBSCAN labels (-1 = noise) and membership probabilities of a (n-1) x 4
+ * single-linkage tree (HOST memory), scikit-learn 1.9 extraction semantics.
+ * method: 0 excess of mass, 1 leaf; maxClusterSize <= 0 means no limit.
+ * Replaces the NumPy extraction of reference python/cuhc/_hdbscan.py:148-350
+ * (no counterpart in its C ABI). */
+int cuhc_hdbscan_labels(const double *tree, long long n, long long minClusterSize, int method,
+                        int allowSingleCluster, double epsilon, long long maxClusterSize,
+                        long long *labels, double *probabilities);
+
 /* Tensor-core screening of the all-pairs passes: 0 auto (on for euclidean and
  * sqeuclidean up to 32 features), 1 on where supported, 2 off. Results never
  * change; returns CUHC_ERROR_INVALID_ALGORITHM for other values. */
