@@ -32,7 +32,8 @@ enum PruneMode : int { kPruneAuto = 0, kPruneAlways = 1, kPruneNever = 2 };
 enum CoreMethod : int { kCoreAuto = 0, kCoreFused = 1, kCoreRadix = 2 };
 constexpr int kMaxFusedK = 64;     // reference hdbscan.cuh:112
 constexpr int kMaxPruneFeatures = 256;
-// Largest k whose per-row lists fit in shared memory (128 rows x k floats).
+// Largest k whose per-row lists fit in shared memory (128 rows x k floats);
+// larger k uses radix select.
 constexpr int kMaxListK = 256;
 
 std::atomic<int> gPruneMode{kPruneAuto};
@@ -124,7 +125,7 @@ int singleLinkageMst(const float *devPoints, int n, int d, const Metric &m, doub
 
 template <class Metric>
 int hdbscanTree(const float *devPoints, int n, int d, const Metric &m, int minSamples, float alpha,
-                double *hostTree, float *hostCore, cudaStream_t s) {
+                int coreMethod, double *hostTree, float *hostCore, cudaStream_t s) {
   StatusChain st;
   SpatialIndex index;
   const bool prune = shouldPrune<Metric>(n, d);
@@ -132,7 +133,12 @@ int hdbscanTree(const float *devPoints, int n, int d, const Metric &m, int minSa
   DeviceBuffer<float> core, coreOrig;
   CUHC_TRY(st, core.allocate(paddedToTiles(n), s));
   PassStats stats;
-  CUHC_TRY(st, coreDistances<Metric>(index, m, minSamples, prune, core.get(), &stats, s));
+  // Radix select when asked for, or when the per-row lists would not fit
+  // shared memory (the reference's Auto picks radix above k = 64).
+  if (coreMethod == kCoreRadix || minSamples > kMaxListK)
+    CUHC_TRY(st, coreDistancesRadix<Metric>(index, m, minSamples, core.get(), s));
+  else
+    CUHC_TRY(st, coreDistances<Metric>(index, m, minSamples, prune, core.get(), &stats, s));
   CUHC_TRY(st, index.updateMinValues(core.get()));
   DeviceEdges edges;
   MutualReachWeight weight;
@@ -200,8 +206,6 @@ int validateHdbscan(int n, int d, int minSamples, int coreMethod) {
     return kErrorInvalidShape;
   if (coreMethod < 0 || coreMethod > 2 || (coreMethod == kCoreFused && minSamples > kMaxFusedK))
     return kErrorInvalidAlgorithm;
-  if (minSamples > kMaxListK)
-    return kErrorTooLarge;
   return 0;
 }
 
@@ -297,7 +301,8 @@ int cuhc_hdbscan_tree(const float *hostPoints, int n, int d, int metricId, float
                                ctx.stream));
   if (st.ok())
     st(withMetric(metricId, p, [&](auto m) {
-      return hdbscanTree(points.get(), n, d, m, minSamples, alpha, hostTree, hostCore, ctx.stream);
+      return hdbscanTree(points.get(), n, d, m, minSamples, alpha, coreMethod, hostTree, hostCore,
+                         ctx.stream);
     }));
   return st.code;
 }
@@ -385,7 +390,8 @@ int cuhc_hdbscan_tree_device(const float *devicePoints, int n, int d, int metric
   st(ctx.status);
   if (st.ok())
     st(withMetric(metricId, p, [&](auto m) {
-      return hdbscanTree(devicePoints, n, d, m, minSamples, alpha, hostTree, hostCore, ctx.stream);
+      return hdbscanTree(devicePoints, n, d, m, minSamples, alpha, coreMethod, hostTree, hostCore,
+                         ctx.stream);
     }));
   return st.code;
 }

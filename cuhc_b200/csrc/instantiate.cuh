@@ -4,6 +4,7 @@
 
 #include "boruvka.cuh"
 #include "pairwise.cuh"
+#include "radix.cuh"
 
 namespace cuhc {
 
@@ -32,5 +33,7 @@ int pairwiseDistances(const float *A, int nA, const float *B, int nB, int d, con
       cuhc::PassStats *, cudaStream_t);                                                            \
   template int cuhc::coreDistances<M>(cuhc::SpatialIndex &, const M &, int, bool, float *,         \
                                       cuhc::PassStats *, cudaStream_t);                            \
+  template int cuhc::coreDistancesRadix<M>(cuhc::SpatialIndex &, const M &, int, float *,        \
+                                           cudaStream_t);                                        \
   template int cuhc::pairwiseDistances<M>(const float *, int, const float *, int, int, const M &,  \
                                           float *, cudaStream_t);

@@ -50,4 +50,11 @@ template <class Metric>
 int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, float *core,
                   PassStats *stats, cudaStream_t stream);
 
+// The same core distances for any 1 <= k <= n by radix select over chunks of
+// the materialised distance matrix (radix.cuh). Bit-identical to
+// coreDistances.
+template <class Metric>
+int coreDistancesRadix(SpatialIndex &index, const Metric &metric, int k, float *core,
+                       cudaStream_t stream);
+
 } // namespace cuhc
