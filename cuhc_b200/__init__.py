@@ -5,10 +5,12 @@ A drop-in for the Python API of cuhc (scipy / scikit-learn semantics):
 `pairwise_distances`, over the C ABI of libcuhc.so (include/cuhc.h).
 """
 
+from ._batch import batched_trees
 from ._distances import METRIC_IDS, pairwise_distances
 from ._linkage import LINKAGE_IDS, fcluster, linkage
 
-__all__ = ["LINKAGE_IDS", "METRIC_IDS", "fcluster", "linkage", "pairwise_distances"]
+__all__ = ["LINKAGE_IDS", "METRIC_IDS", "batched_trees", "fcluster", "linkage",
+           "pairwise_distances"]
 
 try:  # estimators need scikit-learn
     from ._estimators import AgglomerativeClustering  # noqa: F401

@@ -204,27 +204,38 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
   p.tilesComputed = tiles.get();
   p.error = error.get();
   p.screenStats = screenCounters();
+  p.rootOfTile = index.numInstances > 1 ? index.rootOfTile.get() : nullptr;
 
   const bool screened = useScreen<Metric>(index.d, 0) && index.extentsWithin(kScreenMaxExtent);
   int numComponents = n, totalEdges = 0, rounds = 0;
   unsigned long long tilesSoFar = 0;
   int hostCounters[4];
-  while (st.ok() && numComponents > 1) {
-    CUHC_TRY(st, index.updatePurity(comp.get()));
+  // Each instance of a batch ends as one component; padding slots stay
+  // components of their own.
+  const int finalComponents = index.numInstances + index.numPads;
+  int maxJumps = 1;
+  while ((1 << maxJumps) < n)
+    ++maxJumps;
+  // One round, enqueued on the stream with no host work: counters[0] counts
+  // every edge so far (edges are written at absolute slots), counters[1..2]
+  // this round's roots and unjumped parents.
+  auto enqueueRound = [&](bool first, int jumps, bool timed) {
+    StatusChain rs;
+    CUHC_TRY(rs, index.updatePurity(comp.get()));
     fillU32<<<blocks(n), 256, 0, stream>>>(compBest.get(), 0x7f800000u, n); noteLaunch();
-    if (rounds > 0) {
+    if (!first) {
       seedComponentBest<<<blocks(n), 256, 0, stream>>>(nearest.get(), index.rank.get(),
                                                        comp.get(), compBest.get(), n);
       noteLaunch();
     }
-    CUHC_TRY(st, cudaGetLastError());
-    p.singletons = rounds == 0;
+    CUHC_TRY(rs, cudaGetLastError());
+    p.singletons = first;
     {
-      PassTimer timer(screened ? kTimerScreenPass : kTimerNearestPass, stream);
+      PassTimer timer(timed ? (screened ? kTimerScreenPass : kTimerNearestPass) : -1, stream);
       if (screened)
-        CUHC_TRY(st, (launchScreen<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
+        CUHC_TRY(rs, (launchScreen<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
       else
-        CUHC_TRY(st, (launchPass<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
+        CUHC_TRY(rs, (launchPass<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
       if (timer.start) {
         unsigned long long tilesNow = 0;
         cudaMemcpyAsync(&tilesNow, tiles.get(), sizeof(tilesNow), cudaMemcpyDeviceToHost, stream);
@@ -232,27 +243,51 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
         tilesSoFar = tilesNow;
       }
     }
-    CUHC_TRY(st, cudaMemsetAsync(compKey.get(), 0xff, n * sizeof(unsigned long long), stream));
-    CUHC_TRY(st, cudaMemsetAsync(compV.get(), 0xff, n * sizeof(unsigned int), stream));
-    CUHC_TRY(st, cudaMemsetAsync(counters.get(), 0, 4 * sizeof(int), stream));
+    CUHC_TRY(rs, cudaMemsetAsync(compKey.get(), 0xff, n * sizeof(unsigned long long), stream));
+    CUHC_TRY(rs, cudaMemsetAsync(compV.get(), 0xff, n * sizeof(unsigned int), stream));
+    CUHC_TRY(rs, cudaMemsetAsync(counters.get() + 1, 0, 2 * sizeof(int), stream));
     componentKeyPass1<<<blocks(n), 256, 0, stream>>>(nearest.get(), index.order.get(), comp.get(),
                                                      compKey.get(), n); noteLaunch();
     componentKeyPass2<<<blocks(n), 256, 0, stream>>>(nearest.get(), index.order.get(), comp.get(),
                                                      compKey.get(), compV.get(), n); noteLaunch();
     hookComponents<<<blocks(n), 256, 0, stream>>>(
-        comp.get(), index.rank.get(), compKey.get(), compV.get(), parent.get(),
-        edges.u.get() + totalEdges, edges.v.get() + totalEdges, edges.w.get() + totalEdges,
-        counters.get(), n - 1 - totalEdges, n); noteLaunch();
-    int jumps = 1;
-    while ((1 << jumps) < numComponents)
-      ++jumps;
-    for (int j = 0; j <= jumps; ++j) {
+        comp.get(), index.rank.get(), compKey.get(), compV.get(), parent.get(), edges.u.get(),
+        edges.v.get(), edges.w.get(), counters.get(), n - 1, n); noteLaunch();
+    for (int jmp = 0; jmp <= jumps; ++jmp) {
       jumpParents<<<blocks(n), 256, 0, stream>>>(comp.get(), parent.get(), n);
       noteLaunch();
     }
     countRoots<<<blocks(n), 256, 0, stream>>>(comp.get(), parent.get(), counters.get(), n); noteLaunch();
     relabel<<<blocks(n), 256, 0, stream>>>(comp.get(), parent.get(), n); noteLaunch();
-    CUHC_TRY(st, cudaGetLastError());
+    CUHC_TRY(rs, cudaGetLastError());
+    return rs.code;
+  };
+  // Batches replay rounds after the first as one captured CUDA graph (the
+  // round's launches and memsets with the largest jump count, extra jumps
+  // being no-ops); timing needs events between launches and runs eagerly.
+  const bool useGraph = index.numInstances > 1 && !timingEnabled();
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graphExec = nullptr;
+  CUHC_TRY(st, cudaMemsetAsync(counters.get(), 0, 4 * sizeof(int), stream));
+  while (st.ok() && numComponents > finalComponents) {
+    if (useGraph && rounds > 0) {
+      if (!graphExec) {
+        CUHC_TRY(st, cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed));
+        const int captured = enqueueRound(false, maxJumps, false);
+        const cudaError_t ended = cudaStreamEndCapture(stream, &graph);
+        CUHC_TRY(st, captured);
+        CUHC_TRY(st, ended);
+        CUHC_TRY(st, cudaGraphInstantiate(&graphExec, graph, 0));
+        if (!st.ok())
+          break;
+      }
+      CUHC_TRY(st, cudaGraphLaunch(graphExec, stream));
+    } else {
+      int jumps = 1;
+      while ((1 << jumps) < numComponents)
+        ++jumps;
+      CUHC_TRY(st, enqueueRound(rounds == 0, jumps, true));
+    }
     int passError = 0;
     CUHC_TRY(st, cudaMemcpyAsync(hostCounters, counters.get(), 4 * sizeof(int),
                                  cudaMemcpyDeviceToHost, stream));
@@ -266,7 +301,7 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
       st(passError);
       break;
     }
-    const int added = hostCounters[0];
+    const int added = hostCounters[0] - totalEdges;
     if (hostCounters[2] != 0) {
       st(kErrorTimeout);
       break;
@@ -275,13 +310,17 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
       st(kErrorDisconnected);
       break;
     }
-    totalEdges += added;
+    totalEdges = hostCounters[0];
     numComponents = hostCounters[1];
     if (totalEdges > n - 1) {
       st(kErrorNonFinite);
       break;
     }
   }
+  if (graphExec)
+    cudaGraphExecDestroy(graphExec);
+  if (graph)
+    cudaGraphDestroy(graph);
   int err = 0;
   unsigned long long tileCount = 0;
   CUHC_TRY(st, cudaMemcpyAsync(&err, error.get(), sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -302,7 +341,7 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
 
 template <class Metric>
 int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, float *core,
-                  PassStats *stats, cudaStream_t stream) {
+                  PassStats *stats, cudaStream_t stream, const int *coreRank) {
   StatusChain st;
   DeviceBuffer<unsigned long long> tiles;
   DeviceBuffer<int> error;
@@ -331,9 +370,11 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
   p.prune = prune;
   p.core = core;
   p.k = k;
+  p.coreRank = coreRank;
   p.tilesComputed = tiles.get();
   p.error = error.get();
   p.screenStats = screenCounters();
+  p.rootOfTile = index.numInstances > 1 ? index.rootOfTile.get() : nullptr;
   {
     const bool screened =
         useScreen<Metric>(index.d, k) && index.extentsWithin(kScreenMaxExtent);
@@ -364,6 +405,51 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
     stats->passes += 1;
   }
   return st.code;
+}
+
+// Device milliseconds of the k-NN pass restricted to the first sampleTiles
+// row tiles, screened or plain (the batched path's autotuner); writes the
+// core distances of those rows only.
+template <class Metric>
+float timeKnnSample(SpatialIndex &index, const Metric &metric, int k, bool screened,
+                    int sampleTiles, float *core, cudaStream_t stream) {
+  PassParams p{};
+  p.tiled = index.tiled.get();
+  p.n = index.n;
+  p.d = index.d;
+  p.numChunks = index.numChunks;
+  p.numTiles = std::min(sampleTiles, index.numTiles);
+  p.order = index.order.get();
+  p.nodeLeft = index.nodeLeft.get();
+  p.nodeRight = index.nodeRight.get();
+  p.nodeFirstTile = index.nodeFirstTile.get();
+  p.leafOfTile = index.leafOfTile.get();
+  p.nodeLow = index.nodeLow.get();
+  p.nodeHigh = index.nodeHigh.get();
+  p.prune = true;
+  p.core = core;
+  p.k = k;
+  p.rootOfTile = index.numInstances > 1 ? index.rootOfTile.get() : nullptr;
+  cudaEvent_t start, stop;
+  cudaEventCreate(&start);
+  cudaEventCreate(&stop);
+  cudaEventRecord(start, stream);
+  const int status =
+      screened ? launchScreen<Metric, PlainWeight, true>(p, metric, PlainWeight{}, index.kc, stream)
+               : launchPass<Metric, PlainWeight, true>(p, metric, PlainWeight{}, index.kc, stream);
+  cudaEventRecord(stop, stream);
+  cudaEventSynchronize(stop);
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, start, stop);
+  cudaEventDestroy(start);
+  cudaEventDestroy(stop);
+  return status == 0 ? ms : INFINITY;
+}
+
+// Whether this index's passes can run screened (metric, width, shared
+// memory, data extent), ignoring the screen mode's "off".
+template <class Metric> bool screenable(SpatialIndex &index, int k) {
+  return useScreen<Metric>(index.d, k) && index.extentsWithin(kScreenMaxExtent);
 }
 
 } // namespace cuhc

@@ -9,7 +9,9 @@
 // The other functions are additions with no counterpart in the reference:
 // device-pointer variants (inputs already in HBM, for callers that keep data
 // on the GPU) and extended pass statistics.
+#include <algorithm>
 #include <atomic>
+#include <map>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -43,7 +45,9 @@ PassStats gStats;
 int currentPruneMode() { return gPruneMode.load(); }
 
 std::atomic<int> gScreenMode{0};
-int currentScreenMode() { return gScreenMode.load(); }
+// Set by the batched path's autotuner for the duration of one call.
+thread_local int tScreenOverride = -1;
+int currentScreenMode() { return tScreenOverride >= 0 ? tScreenOverride : gScreenMode.load(); }
 
 int pairwiseIntoMatrix(const float *points, int n, int d, int metricId, float p, float *out,
                        cudaStream_t s) {
@@ -97,7 +101,7 @@ struct CallContext {
 __global__ void scatterByOrder(const float *__restrict__ byPosition, const int *__restrict__ order,
                                float *__restrict__ byOriginal, int n) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < n)
+  if (p < n && order[p] >= 0) // padding slots of a batch hold no point
     byOriginal[order[p]] = byPosition[p];
 }
 
@@ -162,6 +166,130 @@ int hdbscanTree(const float *devPoints, int n, int d, const Metric &m, int minSa
       st(kErrorDisconnected);
     if (st.ok())
       treeFromOrderedMerges(u, v, w, n, hostTree);
+  }
+  CUHC_TRY(st, cudaStreamSynchronize(s));
+  addStats(stats);
+  return st.code;
+}
+
+// ---- batched trees (many instances, one solve per call) ----
+
+// Autotuner of the batched path: for (metric, d) the faster of the screened
+// and the plain k-NN kernel, timed once per process on the first 2 x SMs row
+// tiles of a batch (after one warm-up launch of each). The choice changes
+// time only, never a result. Returns the screen mode to use (1 on, 2 off).
+std::mutex gTuneMutex;
+std::map<std::pair<int, int>, int> gTuned;
+
+template <class Metric>
+int tuneScreen(SpatialIndex &index, const Metric &m, int metricId, int k, float *scratch,
+               cudaStream_t s) {
+  if (gScreenMode.load() != 0)
+    return gScreenMode.load();
+  if (!screenable<Metric>(index, k))
+    return 2;
+  const std::pair<int, int> key(metricId, index.d);
+  {
+    std::lock_guard<std::mutex> lock(gTuneMutex);
+    const auto it = gTuned.find(key);
+    if (it != gTuned.end())
+      return it->second;
+  }
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const int sample = 2 * sms;
+  float best[2] = {INFINITY, INFINITY};
+  for (int rep = 0; rep < 3; ++rep)
+    for (int v = 0; v < 2; ++v) {
+      const float ms = timeKnnSample(index, m, k, v == 0, sample, scratch, s);
+      if (rep > 0)
+        best[v] = std::min(best[v], ms);
+    }
+  const int mode = best[0] <= best[1] ? 1 : 2;
+  std::lock_guard<std::mutex> lock(gTuneMutex);
+  gTuned[key] = mode;
+  return mode;
+}
+
+struct ScreenOverride {
+  explicit ScreenOverride(int mode) { tScreenOverride = mode; }
+  ~ScreenOverride() { tScreenOverride = -1; }
+};
+
+template <class Metric>
+int batchTrees(const float *devPoints, const std::vector<int> &sizes,
+               const std::vector<long long> &offsets, int d, const Metric &m, int metricId,
+               const int *minSamples, double *hostTrees, float *hostCore, cudaStream_t s) {
+  StatusChain st;
+  SpatialIndex index;
+  CUHC_TRY(st, index.buildBatch(devPoints, sizes, d, s));
+  if (!st.ok())
+    return st.code;
+  const int count = (int)sizes.size(), positions = index.n;
+  int maxK = 0;
+  std::vector<int> hostRank(positions, 0);
+  for (int i = 0; i < count; ++i) {
+    maxK = std::max(maxK, minSamples[i]);
+    const int base = index.instanceFirstTile[i] * kTile;
+    std::fill(hostRank.begin() + base, hostRank.begin() + base + sizes[i], minSamples[i]);
+  }
+  DeviceBuffer<float> core;
+  DeviceBuffer<int> rank;
+  CUHC_TRY(st, core.allocate(paddedToTiles(positions), s));
+  CUHC_TRY(st, rank.allocate(positions, s));
+  CUHC_TRY(st, cudaMemsetAsync(core.get(), 0, core.bytes(), s));
+  CUHC_TRY(st, cudaMemcpyAsync(rank.get(), hostRank.data(), positions * sizeof(int),
+                               cudaMemcpyHostToDevice, s));
+  CUHC_TRY(st, cudaStreamSynchronize(s));
+  if (!st.ok())
+    return st.code;
+  ScreenOverride screen(tuneScreen(index, m, metricId, std::max(maxK, 1), core.get(), s));
+  CUHC_TRY(st, cudaMemsetAsync(core.get(), 0, core.bytes(), s));
+  PassStats stats;
+  // Mutual reachability with core 0 is the plain distance (keys clamp at 0),
+  // so single-linkage instances (rank 0) share the solve with HDBSCAN ones.
+  if (maxK > 0)
+    CUHC_TRY(st, coreDistances<Metric>(index, m, maxK, true, core.get(), &stats, s, rank.get()));
+  CUHC_TRY(st, index.updateMinValues(core.get()));
+  MutualReachWeight weight;
+  weight.value = core.get();
+  weight.alpha = 1.0f;
+  DeviceEdges edges;
+  CUHC_TRY(st, (boruvkaMst<Metric, MutualReachWeight>(index, m, weight, true, edges, &stats, s)));
+  std::vector<int> u, v;
+  std::vector<float> w;
+  CUHC_TRY(st, sortEdgesToHost(edges, edges.count, s, u, v, w));
+  if (st.ok() && (long long)u.size() != offsets[count] - count)
+    st(kErrorDisconnected);
+  if (st.ok()) {
+    // Edges in (w, u, v) order; each instance's keep that order in local ids.
+    std::vector<std::vector<int>> iu(count), iv(count);
+    std::vector<std::vector<float>> iw(count);
+    for (size_t e = 0; e < u.size(); ++e) {
+      const int i = (int)(std::upper_bound(offsets.begin(), offsets.end(), (long long)u[e]) -
+                          offsets.begin()) - 1;
+      iu[i].push_back(u[e] - (int)offsets[i]);
+      iv[i].push_back(v[e] - (int)offsets[i]);
+      iw[i].push_back(w[e]);
+    }
+    for (int i = 0; i < count && st.ok(); ++i) {
+      if ((int)iu[i].size() != sizes[i] - 1) {
+        st(kErrorDisconnected);
+        break;
+      }
+      treeFromOrderedMerges(iu[i], iv[i], iw[i], sizes[i], hostTrees + (offsets[i] - i) * 4);
+    }
+  }
+  if (hostCore && st.ok()) {
+    DeviceBuffer<float> coreOrig;
+    CUHC_TRY(st, coreOrig.allocate(index.numPoints, s));
+    scatterByOrder<<<(positions + 255) / 256, 256, 0, s>>>(core.get(), index.order.get(),
+                                                           coreOrig.get(), positions);
+    noteLaunch();
+    CUHC_TRY(st, cudaGetLastError());
+    CUHC_TRY(st, cudaMemcpyAsync(hostCore, coreOrig.get(), index.numPoints * sizeof(float),
+                                 cudaMemcpyDeviceToHost, s));
   }
   CUHC_TRY(st, cudaStreamSynchronize(s));
   addStats(stats);
@@ -311,6 +439,43 @@ long long cuhc_condense_tree(const double *tree, long long n, long long minClust
                              long long capacity, long long *parent, long long *child,
                              double *lambda, long long *size) {
   return condenseTree(tree, n, minClusterSize, capacity, parent, child, lambda, size);
+}
+
+int cuhc_trees_batched(const float *hostPoints, const long long *offsets, int count, int d,
+                       int metricId, float p, const int *minSamples, double *trees,
+                       float *core) {
+  if (count < 1 || d < 1 || !offsets || !minSamples || offsets[0] != 0)
+    return kErrorInvalidShape;
+  std::vector<int> sizes(count);
+  std::vector<long long> off(offsets, offsets + count + 1);
+  long long positions = 0;
+  for (int i = 0; i < count; ++i) {
+    const long long n = offsets[i + 1] - offsets[i];
+    if (n < 1 || minSamples[i] < 0 || minSamples[i] > n)
+      return kErrorInvalidShape;
+    sizes[i] = (int)n;
+    positions += (long long)numTilesFor((int)std::min<long long>(n, 1 << 30)) * kTile;
+  }
+  if (positions > (1LL << 30) || offsets[count] * (long long)d > (1LL << 40))
+    return kErrorTooLarge;
+  for (int i = 0; i < count; ++i)
+    if (minSamples[i] > kMaxListK)
+      return kErrorTooLarge;
+  if (metricId < kEuclidean || metricId > kCosine)
+    return kErrorInvalidMetric;
+  CallContext ctx;
+  StatusChain st;
+  st(ctx.status);
+  DeviceBuffer<float> points;
+  CUHC_TRY(st, points.allocate((size_t)offsets[count] * d, ctx.stream));
+  CUHC_TRY(st, cudaMemcpyAsync(points.get(), hostPoints, points.bytes(), cudaMemcpyHostToDevice,
+                               ctx.stream));
+  if (st.ok())
+    st(withMetric(metricId, p, [&](auto m) {
+      return batchTrees(points.get(), sizes, off, d, m, metricId, minSamples, trees, core,
+                        ctx.stream);
+    }));
+  return st.code;
 }
 
 int cuhc_set_pruning(int mode) {

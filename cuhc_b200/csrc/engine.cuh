@@ -157,6 +157,8 @@ struct PassParams {
   unsigned long long *tilesComputed;
   int *error;
   unsigned long long *screenStats; // ScreenCounter sums (null: not counted)
+  const int *rootOfTile;  // traversal root per row tile (null: node 0)
+  const int *coreRank;    // knn-mode rank per position, 0 = core 0 (null: k for all)
 };
 
 // Lower bound of every distance between the row tile box (shared memory)

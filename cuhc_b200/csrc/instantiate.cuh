@@ -32,7 +32,10 @@ int pairwiseDistances(const float *A, int nA, const float *B, int nB, int d, con
       cuhc::SpatialIndex &, const M &, const cuhc::MutualReachWeight &, bool, cuhc::DeviceEdges &, \
       cuhc::PassStats *, cudaStream_t);                                                            \
   template int cuhc::coreDistances<M>(cuhc::SpatialIndex &, const M &, int, bool, float *,         \
-                                      cuhc::PassStats *, cudaStream_t);                            \
+                                      cuhc::PassStats *, cudaStream_t, const int *);                            \
+  template bool cuhc::screenable<M>(cuhc::SpatialIndex &, int);                                    \
+  template float cuhc::timeKnnSample<M>(cuhc::SpatialIndex &, const M &, int, bool, int, float *,  \
+                                        cudaStream_t);                                           \
   template int cuhc::coreDistancesRadix<M>(cuhc::SpatialIndex &, const M &, int, float *,        \
                                            cudaStream_t);                                        \
   template int cuhc::pairwiseDistances<M>(const float *, int, const float *, int, int, const M &,  \

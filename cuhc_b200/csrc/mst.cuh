@@ -48,11 +48,17 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
 // Exact core distances (k-th nearest, the point itself first) by position.
 template <class Metric>
 int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, float *core,
-                  PassStats *stats, cudaStream_t stream);
+                  PassStats *stats, cudaStream_t stream, const int *coreRank = nullptr);
 
 // The same core distances for any 1 <= k <= n by radix select over chunks of
 // the materialised distance matrix (radix.cuh). Bit-identical to
 // coreDistances.
+template <class Metric> bool screenable(SpatialIndex &index, int k);
+
+template <class Metric>
+float timeKnnSample(SpatialIndex &index, const Metric &metric, int k, bool screened,
+                    int sampleTiles, float *core, cudaStream_t stream);
+
 template <class Metric>
 int coreDistancesRadix(SpatialIndex &index, const Metric &metric, int k, float *core,
                        cudaStream_t stream);

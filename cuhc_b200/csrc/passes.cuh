@@ -75,7 +75,7 @@ __device__ __forceinline__ void refreshThresholds(const PassParams &p, const Met
   float t = -INFINITY;
   if (tid < kTile) {
     const int pos = firstRow + tid;
-    const bool valid = pos < p.n;
+    const bool valid = pos < p.n && p.order[pos] >= 0; // padding slots never search
     float thr, filter = -INFINITY;
     if (kKnn) {
       thr = lists[tid * p.k + p.k - 1];
@@ -194,7 +194,7 @@ template <class Metric>
 __device__ __forceinline__ void knnEpilogue(const Metric &m, const PassState &sh, float *lists,
                                             int k, typename Metric::Acc (&acc)[8][8],
                                             int firstRow, int firstCol, int n,
-                                            const TileGeom &g) {
+                                            const int *colOrig, const TileGeom &g) {
   const int lane = threadIdx.x & 31;
   const unsigned groupMask = (lane < 16) ? 0x0000ffffu : 0xffff0000u;
 #pragma unroll
@@ -213,7 +213,7 @@ __device__ __forceinline__ void knnEpilogue(const Metric &m, const PassState &sh
     if (rowPos < n) {
 #pragma unroll
       for (int c = 0; c < 8; ++c)
-        if (firstCol + g.col(c) < n && m.filter(acc[r][c]) <= F)
+        if (firstCol + g.col(c) < n && colOrig[g.col(c)] >= 0 && m.filter(acc[r][c]) <= F)
           pending |= 1u << c;
     }
     while (true) {
@@ -401,9 +401,10 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
     fenceBarrierInit();
     sh.frontLen = 0;
     sh.overflow = 0;
-    const int rootPure = (!kKnn && p.nodePure) ? p.nodePure[0] : -1;
+    const int root = p.rootOfTile ? p.rootOfTile[I] : 0;
+    const int rootPure = (!kKnn && p.nodePure) ? p.nodePure[root] : -1;
     if (!(rowPure >= 0 && rootPure == rowPure)) {
-      sh.frontNode[0] = 0;
+      sh.frontNode[0] = root;
       sh.frontLen = 1;
     }
   }
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
         acc[r][c] = m.init();
     accumulateChunk<Metric, KC>(sA, bTile, m, acc, g);
     if (kKnn)
-      knnEpilogue(m, sh, lists, p.k, acc, firstRow, J * kTile, p.n, g);
+      knnEpilogue(m, sh, lists, p.k, acc, firstRow, J * kTile, p.n, cm.orig, g);
     else
       nearestEpilogue<Metric, Weight>(m, w, sh, cm, acc, rowComp, rowVal, J * kTile, p.n,
                                       useComp, useValue,
@@ -460,7 +461,7 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
     typename Metric::Acc acc[8][8];
     computeTile<Metric, KC>(p.tiled, p.tiled, p.numChunks, I, J, sA, sB[0], m, acc, g);
     if (kKnn)
-      knnEpilogue(m, sh, lists, p.k, acc, firstRow, J * kTile, p.n, g);
+      knnEpilogue(m, sh, lists, p.k, acc, firstRow, J * kTile, p.n, meta[0].orig, g);
     else
       nearestEpilogue<Metric, Weight>(m, w, sh, meta[0], acc, rowComp, rowVal, J * kTile, p.n,
                                       useComp, useValue, maskPass, g, sh.rowBest);
@@ -565,10 +566,12 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
   if (tid < kTile) {
     const int pos = firstRow + tid;
     if (pos < p.n) {
-      if (kKnn)
-        p.core[pos] = lists[tid * p.k + p.k - 1];
-      else
+      if (kKnn) {
+        const int rank = p.coreRank ? p.coreRank[pos] : p.k;
+        p.core[pos] = rank > 0 ? lists[tid * p.k + rank - 1] : 0.0f;
+      } else {
         p.nearest[pos] = sh.rowBest[tid];
+      }
     }
   }
   if (tid == 0) {

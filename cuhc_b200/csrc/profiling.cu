@@ -27,8 +27,8 @@ unsigned long long *screenCounters() {
 }
 
 PassTimer::PassTimer(int k, cudaStream_t s) : kind(k), stream(s) {
-  if (!timingEnabled())
-    return;
+  if (k < 0 || !timingEnabled())
+    return; // kind -1: a launch that is not timed (e.g. inside a stream capture)
   cudaEventCreate(&start);
   cudaEventCreate(&stop);
   cudaEventRecord(start, stream);

@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   // Consumer row state (thread = row).
   const int myRow = tid & (kTile - 1);
   const int myPos = firstRow + myRow;
-  const bool myValid = consumer && myPos < p.n;
+  const bool myValid = consumer && myPos < p.n && p.order[myPos] >= 0; // not a padding slot
   const int myComp = myValid ? (p.component ? p.component[myPos] : p.order[myPos]) : -2;
   const float myVal = myValid ? w.load(myPos) : 0.0f;
   unsigned int *compSlot = (!kKnn && myValid && p.compBest) ? p.compBest + myComp : nullptr;
@@ -261,9 +261,10 @@ __global__ void __launch_bounds__(kThreads, 2)
     ss.rowSetCount = 0;
     sh.frontLen = 0;
     sh.overflow = 0;
-    const int rootPure = (!kKnn && p.nodePure) ? p.nodePure[0] : -1;
+    const int root = p.rootOfTile ? p.rootOfTile[I] : 0;
+    const int rootPure = (!kKnn && p.nodePure) ? p.nodePure[root] : -1;
     if (!(rowPure >= 0 && rootPure == rowPure)) {
-      sh.frontNode[0] = 0;
+      sh.frontNode[0] = root;
       sh.frontLen = 1;
     }
   }
@@ -543,8 +544,8 @@ __global__ void __launch_bounds__(kThreads, 2)
                 const int c = __ffs(candidates) - 1;
                 candidates &= candidates - 1;
                 const int jj = chunk * 32 + c;
-                if (J * kTile + jj >= p.n)
-                  continue;
+                if (J * kTile + jj >= p.n || cOrig[jj] < 0)
+                  continue; // beyond the points, or a padding slot
                 if (!kKnn && (useComp ? cComp[jj] : cOrig[jj]) == myComp)
                   continue;
                 // The reference's exact FP32 distance (zero-padded features add 0).
@@ -617,11 +618,13 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (lastCommit >= 0)
       mbarrierWait(&ss.mmaFull[lastCommit & 1], (lastCommit >> 1) & 1);
   }
-  if (myValid) {
-    if (kKnn)
-      p.core[myPos] = lists[myRow * p.k + p.k - 1];
-    else
+  if (consumer && myPos < p.n) {
+    if (kKnn) {
+      const int rank = myValid ? (p.coreRank ? p.coreRank[myPos] : p.k) : 0;
+      p.core[myPos] = rank > 0 ? lists[myRow * p.k + rank - 1] : 0.0f;
+    } else {
       p.nearest[myPos] = rowBest;
+    }
   }
   if (consumer && p.screenStats) {
     for (int off = 16; off > 0; off /= 2) {

@@ -53,6 +53,75 @@ void BvhTopology::build(int T) {
   levelStart.push_back((int)firstTile.size());
   numNodes = (int)firstTile.size();
   depth = (int)levelStart.size() - 1;
+  spans.assign(numNodes, 0);
+  rootOfInstance.assign(1, 0);
+}
+
+void BvhTopology::buildForest(const std::vector<int> &instanceTiles) {
+  std::vector<int> start(instanceTiles.size() + 1, 0);
+  for (size_t i = 0; i < instanceTiles.size(); ++i)
+    start[i + 1] = start[i] + instanceTiles[i];
+  const int T = start.back();
+  numTiles = T;
+  left.clear();
+  right.clear();
+  firstTile.clear();
+  tileCount.clear();
+  levelStart.clear();
+  spans.clear();
+  leafOfTile.assign(T, -1);
+  rootOfInstance.assign(instanceTiles.size(), -1);
+  // Instance holding a tile: the last start <= tile.
+  auto instanceOf = [&](int tile) {
+    return (int)(std::upper_bound(start.begin(), start.end(), tile) - start.begin()) - 1;
+  };
+  auto addNode = [&](int first, int count) {
+    firstTile.push_back(first);
+    tileCount.push_back(count);
+    left.push_back(-1);
+    right.push_back(-1);
+    spans.push_back(0);
+    return (int)firstTile.size() - 1;
+  };
+  addNode(0, T);
+  levelStart.push_back(0);
+  int begin = 0;
+  while (begin < (int)firstTile.size()) {
+    const int end = (int)firstTile.size();
+    for (int node = begin; node < end; ++node) {
+      const int first = firstTile[node], count = tileCount[node];
+      const int a = instanceOf(first), b = instanceOf(first + count - 1);
+      if (a == b && rootOfInstance[a] < 0)
+        rootOfInstance[a] = node;
+      if (count == 1) {
+        leafOfTile[first] = node;
+        continue;
+      }
+      int leftCount;
+      if (a != b) {
+        // The boundary start[a + 1 .. b] nearest the middle tile.
+        const int middle = first + count / 2;
+        int best = start[a + 1];
+        for (int i = a + 1; i <= b; ++i)
+          if (std::abs(start[i] - middle) < std::abs(best - middle))
+            best = start[i];
+        leftCount = best - first;
+        spans[node] = 1;
+      } else {
+        leftCount = count / 2;
+      }
+      const int l = addNode(first, leftCount);
+      const int r = addNode(first + leftCount, count - leftCount);
+      left[node] = l;
+      right[node] = r;
+    }
+    begin = end;
+    if (begin < (int)firstTile.size())
+      levelStart.push_back(begin);
+  }
+  levelStart.push_back((int)firstTile.size());
+  numNodes = (int)firstTile.size();
+  depth = (int)levelStart.size() - 1;
 }
 
 namespace {
@@ -84,7 +153,10 @@ __global__ void chooseSplitKernel(const float *__restrict__ points, int n, int d
   for (int f = 0; f < d; ++f) {
     float lo = INFINITY, hi = -INFINITY;
     for (int s = lane; s < samples; s += 32) {
-      const float v = points[(size_t)order[a + s * step] * d + f];
+      const int o = order[a + s * step];
+      if (o < 0)
+        continue; // padding slot of a batch
+      const float v = points[(size_t)o * d + f];
       lo = fminf(lo, v);
       hi = fmaxf(hi, v);
     }
@@ -105,10 +177,8 @@ __global__ void chooseSplitKernel(const float *__restrict__ points, int n, int d
 __device__ __forceinline__ int nodeAtDepth(int tile, int level, const int *left, const int *right,
                                            const int *firstTile, const int *tileCount) {
   int node = 0;
-  for (int l = 0; l < level && tileCount[node] > 1; ++l) {
-    const int mid = firstTile[node] + tileCount[node] / 2;
-    node = tile < mid ? left[node] : right[node];
-  }
+  for (int l = 0; l < level && tileCount[node] > 1; ++l)
+    node = tile < firstTile[right[node]] ? left[node] : right[node];
   return node;
 }
 
@@ -120,16 +190,19 @@ __global__ void levelKeysKernel(const float *__restrict__ points, int n, int d, 
                                 const int *__restrict__ right, const int *__restrict__ firstTile,
                                 const int *__restrict__ tileCount,
                                 const int *__restrict__ splitFeature,
+                                const unsigned char *__restrict__ spans,
                                 unsigned long long *__restrict__ keys) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n)
     return;
   const int node = nodeAtDepth(p / kTile, level, left, right, firstTile, tileCount);
   uint32_t low;
-  if (tileCount[node] > 1)
-    low = orderedBits(points[(size_t)order[p] * d + splitFeature[node]]);
+  if (tileCount[node] == 1 || (spans && spans[node]))
+    low = (uint32_t)p; // single tiles and nodes over several instances keep their order
+  else if (order[p] < 0)
+    low = 0xffffffffu; // padding stays behind its instance's points
   else
-    low = (uint32_t)p;
+    low = orderedBits(points[(size_t)order[p] * d + splitFeature[node]]);
   keys[p] = ((unsigned long long)firstTile[node] << 32) | low;
 }
 
@@ -148,6 +221,8 @@ __global__ void gatherTiledKernel(const float *__restrict__ points, int n, int d
   if (p >= n)
     return;
   const int o = order ? order[p] : p;
+  if (o < 0)
+    return; // padding slot of a batch: stays zero
   if (rank)
     rank[o] = p;
   const int t = p / kTile, r = p % kTile;
@@ -160,7 +235,8 @@ __global__ void gatherTiledKernel(const float *__restrict__ points, int n, int d
 // One warp per tile: per-feature min / max over its valid points.
 __global__ void leafBoxKernel(const float *__restrict__ tiled, int n, int d, int kc, int numChunks,
                               int numTiles, const int *__restrict__ leafOfTile,
-                              float *__restrict__ low, float *__restrict__ high) {
+                              const int *__restrict__ padOrder, float *__restrict__ low,
+                              float *__restrict__ high) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) / 32, lane = threadIdx.x % 32;
   if (warp >= numTiles)
     return;
@@ -174,7 +250,7 @@ __global__ void leafBoxKernel(const float *__restrict__ tiled, int n, int d, int
     float lo = INFINITY, hi = -INFINITY;
 #pragma unroll
     for (int i = 0; i < 4; ++i)
-      if (lane * 4 + i < valid) {
+      if (lane * 4 + i < valid && (!padOrder || padOrder[t * kTile + lane * 4 + i] >= 0)) {
         lo = fminf(lo, vals[i]);
         hi = fmaxf(hi, vals[i]);
       }
@@ -258,17 +334,55 @@ int blocksFor(long long work, int threads) { return (int)((work + threads - 1) /
 } // namespace
 
 int SpatialIndex::build(const float *points, int n_, int d_, bool spatial, cudaStream_t s) {
-  n = n_;
+  numInstances = 1;
+  numPads = 0;
+  numPoints = n_;
+  instanceFirstTile.assign(1, 0);
+  topo.build(numTilesFor(n_));
+  return buildCommon(points, n_, d_, spatial, nullptr, s);
+}
+
+int SpatialIndex::buildBatch(const float *points, const std::vector<int> &sizes, int d_,
+                             cudaStream_t s) {
+  numInstances = (int)sizes.size();
+  std::vector<int> tiles(sizes.size());
+  instanceFirstTile.assign(sizes.size(), 0);
+  long long total = 0;
+  int tileSum = 0;
+  for (size_t i = 0; i < sizes.size(); ++i) {
+    tiles[i] = numTilesFor(sizes[i]);
+    instanceFirstTile[i] = tileSum;
+    tileSum += tiles[i];
+    total += sizes[i];
+  }
+  numPoints = (int)total;
+  topo.buildForest(tiles);
+  const int positions = tileSum * kTile;
+  numPads = positions - numPoints;
+  // Instance i's rows start on its first tile; the rest of its last tile is padding.
+  std::vector<int> hostOrder(positions, -1);
+  long long offset = 0;
+  for (size_t i = 0; i < sizes.size(); ++i) {
+    const int base = instanceFirstTile[i] * kTile;
+    for (int j = 0; j < sizes[i]; ++j)
+      hostOrder[base + j] = (int)(offset + j);
+    offset += sizes[i];
+  }
+  return buildCommon(points, positions, d_, true, &hostOrder, s);
+}
+
+int SpatialIndex::buildCommon(const float *points, int positions, int d_, bool spatial,
+                              const std::vector<int> *hostOrder, cudaStream_t s) {
+  n = positions;
   d = d_;
   stream = s;
-  numTiles = numTilesFor(n);
+  numTiles = topo.numTiles;
   kc = chunkWidthFor(d);
   numChunks = numChunksFor(d);
-  topo.build(numTiles);
   StatusChain st;
   const int N = topo.numNodes;
   CUHC_TRY(st, order.allocate(paddedToTiles(n), s));
-  CUHC_TRY(st, rank.allocate(n, s));
+  CUHC_TRY(st, rank.allocate(std::max(numPoints, 1), s));
   CUHC_TRY(st, nodeLeft.allocate(N, s));
   CUHC_TRY(st, nodeRight.allocate(N, s));
   CUHC_TRY(st, nodeFirstTile.allocate(N, s));
@@ -291,7 +405,28 @@ int SpatialIndex::build(const float *points, int n_, int d_, bool spatial, cudaS
                                cudaMemcpyHostToDevice, s));
   CUHC_TRY(st, cudaMemcpyAsync(leafOfTile.get(), topo.leafOfTile.data(), numTiles * sizeof(int),
                                cudaMemcpyHostToDevice, s));
-  iotaKernel<<<blocksFor(n, 256), 256, 0, s>>>(order.get(), n); noteLaunch();
+  if (hostOrder) {
+    CUHC_TRY(st, nodeSpans.allocate(N, s));
+    CUHC_TRY(st, rootOfTile.allocate(numTiles, s));
+    std::vector<int> roots(numTiles);
+    for (int i = 0; i < numInstances; ++i) {
+      const int last = i + 1 < numInstances ? instanceFirstTile[i + 1] : numTiles;
+      for (int t = instanceFirstTile[i]; t < last; ++t)
+        roots[t] = topo.rootOfInstance[i];
+    }
+    CUHC_TRY(st, cudaMemcpyAsync(nodeSpans.get(), topo.spans.data(), N, cudaMemcpyHostToDevice,
+                                 s));
+    CUHC_TRY(st, cudaMemcpyAsync(rootOfTile.get(), roots.data(), numTiles * sizeof(int),
+                                 cudaMemcpyHostToDevice, s));
+    CUHC_TRY(st, cudaMemcpyAsync(order.get(), hostOrder->data(), n * sizeof(int),
+                                 cudaMemcpyHostToDevice, s));
+    // The host vectors go out of scope on return: wait for the copies.
+    CUHC_TRY(st, cudaStreamSynchronize(s));
+  } else {
+    // Positions past the last point are padding (order -1).
+    CUHC_TRY(st, cudaMemsetAsync(order.get(), 0xff, paddedToTiles(n) * sizeof(int), s));
+    iotaKernel<<<blocksFor(n, 256), 256, 0, s>>>(order.get(), n); noteLaunch();
+  }
   CUHC_TRY(st, cudaGetLastError());
 
   if (spatial && topo.depth > 1 && st.ok()) {
@@ -318,7 +453,8 @@ int SpatialIndex::build(const float *points, int n_, int d_, bool spatial, cudaS
           split.get()); noteLaunch();
       levelKeysKernel<<<blocksFor(n, 256), 256, 0, s>>>(
           points, n, d, level, order.get(), nodeLeft.get(), nodeRight.get(), nodeFirstTile.get(),
-          nodeTileCount.get(), split.get(), keys.get()); noteLaunch();
+          nodeTileCount.get(), split.get(), numInstances > 1 ? nodeSpans.get() : nullptr,
+          keys.get()); noteLaunch();
       CUHC_TRY(st, cudaGetLastError());
       CUHC_TRY(st, cub::DeviceRadixSort::SortPairs(temp.get(), tempBytes, keys.get(),
                                                    keysOut.get(), order.get(), valsOut.get(), n,
@@ -364,8 +500,8 @@ int SpatialIndex::retile(const float *pointsByPosition, int newN) {
   }
   const int N = topo.numNodes;
   leafBoxKernel<<<blocksFor((long long)numTiles * 32, 128), 128, 0, stream>>>(
-      tiled.get(), n, d, kc, numChunks, numTiles, leafOfTile.get(), nodeLow.get(),
-      nodeHigh.get()); noteLaunch();
+      tiled.get(), n, d, kc, numChunks, numTiles, leafOfTile.get(),
+      numInstances > 1 ? order.get() : nullptr, nodeLow.get(), nodeHigh.get()); noteLaunch();
   for (int level = topo.depth - 1; level >= 0; --level) {
     const int lb = topo.levelStart[level], le = topo.levelStart[level + 1];
     internalBoxKernel<<<blocksFor((long long)(le - lb) * d, 256), 256, 0, stream>>>(

@@ -31,7 +31,14 @@ struct BvhTopology {
   // level left to right, so every level is a contiguous node range).
   std::vector<int> left, right, firstTile, tileCount, levelStart;
   std::vector<int> leafOfTile;
+  std::vector<unsigned char> spans; // node holds tiles of several instances
+  std::vector<int> rootOfInstance;  // node whose tiles are exactly the instance's
+  // One instance: balanced halves (left child floor(count / 2) tiles).
   void build(int numTiles);
+  // Consecutive instances of instanceTiles[i] tiles each: a node holding
+  // several instances splits at the instance boundary nearest its middle
+  // tile; inside an instance, balanced halves as in build().
+  void buildForest(const std::vector<int> &instanceTiles);
 };
 
 struct SpatialIndex {
@@ -45,12 +52,26 @@ struct SpatialIndex {
   DeviceBuffer<float> nodeMinValue;      // numNodes
   DeviceBuffer<int> nodePure;            // numNodes: component if pure, else -1
   bool hasMinValues = false;             // nodeMinValue filled by updateMinValues
+  // Batches of instances (buildBatch): each instance starts on a fresh tile;
+  // the slots after its last point are padding (order == -1). n counts every
+  // position then, padding included.
+  int numInstances = 1, numPads = 0, numPoints = 0;
+  std::vector<int> instanceFirstTile;    // host, per instance
+  DeviceBuffer<int> rootOfTile;          // traversal root per tile (batches)
+  DeviceBuffer<unsigned char> nodeSpans; // batches
 
   size_t tileFloats() const { return (size_t)numChunks * kc * kTile; }
 
   // Builds everything from points (n x d row-major, original order, device).
   // spatial=false keeps the original order (positions == original indices).
   int build(const float *points, int n, int d, bool spatial, cudaStream_t stream);
+  // Builds one index over a batch of instances: sizes[i] consecutive rows of
+  // points each (original order), every instance its own k-d tree and BVH
+  // subtree (rootOfTile), so traversals never leave their instance.
+  int buildBatch(const float *points, const std::vector<int> &sizes, int d,
+                 cudaStream_t stream);
+  int buildCommon(const float *points, int positions, int d, bool spatial,
+                  const std::vector<int> *hostOrder, cudaStream_t stream);
   // Re-tiles new point data already in position order (RNN centroids after a
   // round), keeping the order arrays; recomputes boxes.
   int retile(const float *pointsByPosition, int n);

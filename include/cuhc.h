@@ -106,6 +106,22 @@ int cuhc_hdbscan_labels(const double *tree, long long n, long long minClusterSiz
                         int allowSingleCluster, double epsilon, long long maxClusterSize,
                         long long *labels, double *probabilities);
 
+/* Trees of many instances in one batched solve (no counterpart in the
+ * reference; its callers make one cuhc_linkage / cuhc_hdbscan_tree call per
+ * instance). Instance i is rows [offsets[i], offsets[i+1]) of the HOST array
+ * points (numFeatures columns, float32); offsets has count + 1 entries,
+ * offsets[0] = 0, every instance at least one row. minSamples[i] = 0 gives
+ * its single-linkage tree, k >= 1 (k <= 256 and <= its rows) HDBSCAN's tree of
+ * mutual reachability with min_samples k, alpha 1. Instance i's tree,
+ * (n_i - 1) x 4 doubles, starts at row offsets[i] - i of `trees`; core (may
+ * be NULL) receives every point's core distance (0 for single linkage). Each
+ * tree is bit-identical to the per-instance call's. All instances share one
+ * k-d forest, one k-NN pass and one Borůvka solve whose rounds after the
+ * first replay as a CUDA graph. */
+int cuhc_trees_batched(const float *points, const long long *offsets, int count, int numFeatures,
+                       int metricId, float metricParam, const int *minSamples, double *trees,
+                       float *core);
+
 /* Tensor-core screening of the all-pairs passes: 0 auto (on for euclidean and
  * sqeuclidean up to 32 features), 1 on where supported, 2 off. Results never
  * change; returns CUHC_ERROR_INVALID_ALGORITHM for other values. */

@@ -123,3 +123,32 @@ def test_condense_tree_reports_capacity():
                                        _ptr(a, i64), _ptr(a.copy(), i64), _ptr(lam, f64),
                                        _ptr(a.copy(), i64))
     assert rows < -4
+
+
+def test_batched_validation_without_gpu():
+    """cuhc_trees_batched rejects bad shapes before touching a GPU."""
+    import ctypes
+    from cuhc_b200 import _batch  # noqa: F401  (declares the argtypes)
+    lib = _lib.lib
+    pts = np.zeros((10, 2), np.float32)
+    tree = np.zeros((10, 4), np.float64)
+    core = np.zeros(10, np.float32)
+
+    def call(offsets, ks, count=None, d=2, metric=0):
+        off = np.asarray(offsets, np.int64)
+        k = np.asarray(ks, np.int32)
+        return lib.cuhc_trees_batched(
+            pts.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+            off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+            len(ks) if count is None else count, d, metric, 2.0,
+            k.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+            tree.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            core.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+
+    assert call([0, 4, 10], [0, 0], count=0) == -2          # no instance
+    assert call([1, 4, 10], [0, 0]) == -2                   # offsets[0] != 0
+    assert call([0, 4, 4], [0, 0]) == -2                    # empty instance
+    assert call([0, 4, 10], [5, 0]) == -2                   # min_samples > rows
+    assert call([0, 4, 10], [-1, 0]) == -2
+    assert call([0, 4, 10], [0, 1], d=0) == -2
+    assert call([0, 4, 10], [0, 1], metric=9) == -1
