@@ -49,6 +49,152 @@ def make_blobs_with_noise(seed=1, n=N_POINTS, d=N_FEATURES, centers=20, noise=0.
     return np.ascontiguousarray(X[rng.permutation(len(X))])
 
 
+def make_batch_instances(count=4096, seed=4):
+    """The batched workload: `count` problems, n = round(exp(U(ln 64, ln 50,000))),
+    d uniform in {2, 8, 32}, 1-12 Gaussian blobs (centres U[-10, 10]^d, std
+    U(0.5, 2.0)) plus 5% uniform noise over their bounding box, float32;
+    alternately single linkage (min_samples 0) and HDBSCAN (min_cluster_size
+    10, so min_samples 10)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(64), np.log(50_000)))))
+        d = int(rng.choice([2, 8, 32]))
+        blobs = int(rng.integers(1, 13))
+        n_noise = int(round(0.05 * n))
+        m = n - n_noise
+        centres = rng.uniform(-10.0, 10.0, (blobs, d))
+        stds = rng.uniform(0.5, 2.0, blobs)
+        label = rng.integers(0, blobs, m)
+        pts = centres[label] + rng.standard_normal((m, d)) * stds[label, None]
+        lo, hi = pts.min(axis=0), pts.max(axis=0)
+        X = np.vstack([pts, rng.uniform(lo, hi, (n_noise, d))]).astype(np.float32)
+        out.append((np.ascontiguousarray(X[rng.permutation(n)]), 0 if i % 2 == 0 else 10))
+    return out
+
+
+def run_batch(args, local_rank):
+    """Batched trees of the mixed workload against one call per instance."""
+    import torch  # noqa: PLC0415
+    sys.path.insert(0, HERE)
+    from cuhc_b200 import _batch, _lib  # noqa: PLC0415,F401
+    lib = _lib.lib
+    i64p, i32p = ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32)
+    f32, f64 = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)
+    lib.cuhc_trees_batched_device.restype = ctypes.c_int
+    lib.cuhc_trees_batched_device.argtypes = [ctypes.c_void_p, i64p, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_float, i32p, f64, f32]
+    inst = make_batch_instances(args.instances)
+    groups = []
+    for d in (2, 8, 32):
+        idx = [i for i, (X, _) in enumerate(inst) if X.shape[1] == d]
+        sizes = np.array([len(inst[i][0]) for i in idx], np.int64)
+        offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        pts = np.ascontiguousarray(np.concatenate([inst[i][0] for i in idx]))
+        ks = np.array([inst[i][1] for i in idx], np.int32)
+        trees = np.empty((int(offsets[-1]) - len(idx), 4), np.float64)
+        core = np.empty(int(offsets[-1]), np.float32)
+        groups.append(dict(d=d, idx=idx, offsets=offsets, pts=pts, dev=torch.from_numpy(pts).cuda(),
+                           ks=ks, trees=trees, core=core))
+
+    def device_step():
+        for g in groups:
+            _lib.check(lib.cuhc_trees_batched_device(
+                ctypes.c_void_p(g["dev"].data_ptr()), g["offsets"].ctypes.data_as(i64p),
+                len(g["idx"]), g["d"], 0, 2.0, g["ks"].ctypes.data_as(i32p),
+                g["trees"].ctypes.data_as(f64), g["core"].ctypes.data_as(f32)))
+
+    def host_step():
+        for g in groups:
+            _lib.check(lib.cuhc_trees_batched(
+                g["pts"].ctypes.data_as(f32), g["offsets"].ctypes.data_as(i64p), len(g["idx"]),
+                g["d"], 0, 2.0, g["ks"].ctypes.data_as(i32p), g["trees"].ctypes.data_as(f64),
+                g["core"].ctypes.data_as(f32)))
+
+    def timed(step, k):
+        times = []
+        for _ in range(k):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            step()
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        return float(np.mean(times))
+
+    for _ in range(args.warmup):
+        device_step()
+    with ClockSampler(local_rank) as clocks:
+        t_dev = timed(device_step, args.steps)
+    _lib.set_timing(True)
+    _lib.kernel_timing()
+    device_step()
+    kt = _lib.kernel_timing()
+    _lib.set_timing(False)
+    t_host = timed(host_step, max(1, min(args.steps, 2)))
+
+    # One call per instance (device-resident points) on every 8th instance.
+    sample = list(range(0, len(inst), 8))
+    where = {}
+    for g in groups:
+        for j, i in enumerate(g["idx"]):
+            where[i] = (g, j)
+    dev = {i: torch.from_numpy(inst[i][0]).cuda() for i in sample}
+    trees = {i: np.empty((len(inst[i][0]) - 1, 4), np.float64) for i in sample}
+    cores = {i: np.empty(len(inst[i][0]), np.float32) for i in sample}
+
+    def per_instance():
+        for i in sample:
+            X, k = inst[i]
+            if k == 0:
+                _lib.check(lib.cuhc_linkage_device(ctypes.c_void_p(dev[i].data_ptr()), len(X),
+                                                   X.shape[1], 0, 2.0, 0, 1,
+                                                   trees[i].ctypes.data_as(f64)))
+            else:
+                _lib.check(lib.cuhc_hdbscan_tree_device(
+                    ctypes.c_void_p(dev[i].data_ptr()), len(X), X.shape[1], 0, 2.0, k, 1.0, 0,
+                    trees[i].ctypes.data_as(f64), cores[i].ctypes.data_as(f32)))
+
+    per_instance()
+    t_per = timed(per_instance, 1)
+    identical = True
+    for i in sample:
+        g, j = where[i]
+        first = int(g["offsets"][j]) - j
+        Z = g["trees"][first:first + len(inst[i][0]) - 1]
+        identical &= bool(np.array_equal(Z, trees[i]))
+        if inst[i][1]:
+            identical &= bool(np.array_equal(g["core"][g["offsets"][j]:g["offsets"][j + 1]],
+                                             cores[i]))
+    count = len(inst)
+    per_rate = len(sample) / t_per
+    line = {
+        "metric": f"batched exact trees, instances/s on 1 B200 ({count:,} mixed single-linkage / "
+                  "HDBSCAN instances, n 64-50k, d 2/8/32)",
+        "value": round(count / t_dev, 1), "unit": "instances/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_dev * 1e3, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{count} instances, seed 4: n log-uniform in [64, 50,000], d in "
+                               "{2, 8, 32}, 1-12 blobs + 5% noise; even instances single "
+                               "linkage, odd HDBSCAN min_samples 10",
+                   "points": int(sum(len(X) for X, _ in inst)),
+                   "timing": "wall clock around synchronised calls (one call per feature count)"},
+        "e2e": {"value": round(count / t_host, 1), "unit": "instances/s",
+                "h2d_bytes_per_step": int(sum(g["pts"].nbytes for g in groups)),
+                "d2h_bytes_per_step": int(sum(g["trees"].nbytes + g["core"].nbytes
+                                              for g in groups))},
+        "per_instance": {"value": round(per_rate, 1), "unit": "instances/s",
+                         "sample": f"every 8th instance ({len(sample)}), one "
+                                   "cuhc_linkage_device / cuhc_hdbscan_tree_device call each",
+                         "batched_speedup": round((count / t_dev) / per_rate, 2)},
+        "identical_sample": identical,
+        "passes": {k: {"ms": round(v[0], 2), "launches": v[1], "tiles": v[2]}
+                   for k, v in kt.items()},
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle samples during the timed region."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -197,6 +343,10 @@ def main():
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--workload", choices=["hdbscan", "batch"], default="hdbscan",
+                        help="hdbscan: the headline tree; batch: many small instances")
+    parser.add_argument("--instances", type=int, default=4096,
+                        help="instances of the batch workload")
     parser.add_argument("--no-plain", action="store_true",
                         help="skip the screening-off comparison step")
     parser.add_argument("--n", type=int, default=N_POINTS,
@@ -213,6 +363,17 @@ def main():
     if world > 1:
         from datetime import timedelta  # noqa: PLC0415
         dist.init_process_group("nccl", timeout=timedelta(minutes=5))
+
+    if args.workload == "batch":
+        if rank == 0 and args.impl == "ours":
+            run_batch(args, local_rank)
+        elif rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched "
+                              "entry point; its per-instance calls are the batch line's "
+                              "per_instance figure"}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     if args.impl == "reference":
         line = run_reference(args, rank, world)

@@ -441,20 +441,22 @@ long long cuhc_condense_tree(const double *tree, long long n, long long minClust
   return condenseTree(tree, n, minClusterSize, capacity, parent, child, lambda, size);
 }
 
-int cuhc_trees_batched(const float *hostPoints, const long long *offsets, int count, int d,
-                       int metricId, float p, const int *minSamples, double *trees,
-                       float *core) {
+namespace {
+// Checks a batch description; sizes receives the instances' row counts.
+int validateBatch(const long long *offsets, int count, int d, int metricId,
+                  const int *minSamples, std::vector<int> &sizes) {
   if (count < 1 || d < 1 || !offsets || !minSamples || offsets[0] != 0)
     return kErrorInvalidShape;
-  std::vector<int> sizes(count);
-  std::vector<long long> off(offsets, offsets + count + 1);
+  sizes.assign(count, 0);
   long long positions = 0;
   for (int i = 0; i < count; ++i) {
     const long long n = offsets[i + 1] - offsets[i];
     if (n < 1 || minSamples[i] < 0 || minSamples[i] > n)
       return kErrorInvalidShape;
+    if (n > (1LL << 30))
+      return kErrorTooLarge;
     sizes[i] = (int)n;
-    positions += (long long)numTilesFor((int)std::min<long long>(n, 1 << 30)) * kTile;
+    positions += (long long)numTilesFor((int)n) * kTile;
   }
   if (positions > (1LL << 30) || offsets[count] * (long long)d > (1LL << 40))
     return kErrorTooLarge;
@@ -463,6 +465,18 @@ int cuhc_trees_batched(const float *hostPoints, const long long *offsets, int co
       return kErrorTooLarge;
   if (metricId < kEuclidean || metricId > kCosine)
     return kErrorInvalidMetric;
+  return 0;
+}
+} // namespace
+
+int cuhc_trees_batched(const float *hostPoints, const long long *offsets, int count, int d,
+                       int metricId, float p, const int *minSamples, double *trees,
+                       float *core) {
+  std::vector<int> sizes;
+  const int invalid = validateBatch(offsets, count, d, metricId, minSamples, sizes);
+  if (invalid)
+    return invalid;
+  std::vector<long long> off(offsets, offsets + count + 1);
   CallContext ctx;
   StatusChain st;
   st(ctx.status);
@@ -473,6 +487,25 @@ int cuhc_trees_batched(const float *hostPoints, const long long *offsets, int co
   if (st.ok())
     st(withMetric(metricId, p, [&](auto m) {
       return batchTrees(points.get(), sizes, off, d, m, metricId, minSamples, trees, core,
+                        ctx.stream);
+    }));
+  return st.code;
+}
+
+int cuhc_trees_batched_device(const float *devicePoints, const long long *offsets, int count,
+                              int d, int metricId, float p, const int *minSamples, double *trees,
+                              float *core) {
+  std::vector<int> sizes;
+  const int invalid = validateBatch(offsets, count, d, metricId, minSamples, sizes);
+  if (invalid)
+    return invalid;
+  std::vector<long long> off(offsets, offsets + count + 1);
+  CallContext ctx;
+  StatusChain st;
+  st(ctx.status);
+  if (st.ok())
+    st(withMetric(metricId, p, [&](auto m) {
+      return batchTrees(devicePoints, sizes, off, d, m, metricId, minSamples, trees, core,
                         ctx.stream);
     }));
   return st.code;

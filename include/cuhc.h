@@ -122,6 +122,11 @@ int cuhc_trees_batched(const float *points, const long long *offsets, int count,
                        int metricId, float metricParam, const int *minSamples, double *trees,
                        float *core);
 
+/* cuhc_trees_batched with the points already in device memory. */
+int cuhc_trees_batched_device(const float *devicePoints, const long long *offsets, int count,
+                              int numFeatures, int metricId, float metricParam,
+                              const int *minSamples, double *trees, float *core);
+
 /* Tensor-core screening of the all-pairs passes: 0 auto (on for euclidean and
  * sqeuclidean up to 32 features), 1 on where supported, 2 off. Results never
  * change; returns CUHC_ERROR_INVALID_ALGORITHM for other values. */
