@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "profiling.cuh"
@@ -263,22 +264,44 @@ int batchTrees(const float *devPoints, const std::vector<int> &sizes,
   if (st.ok() && (long long)u.size() != offsets[count] - count)
     st(kErrorDisconnected);
   if (st.ok()) {
-    // Edges in (w, u, v) order; each instance's keep that order in local ids.
-    std::vector<std::vector<int>> iu(count), iv(count);
-    std::vector<std::vector<float>> iw(count);
-    for (size_t e = 0; e < u.size(); ++e) {
+    // Edges in (w, u, v) order, partitioned stably by instance (instance i's
+    // n_i - 1 edges at slots offsets[i] - i ...), in local ids; then every
+    // instance's tree on the host threads.
+    const size_t edgesTotal = u.size();
+    std::vector<int> lu(edgesTotal), lv(edgesTotal);
+    std::vector<float> lw(edgesTotal);
+    std::vector<long long> fill(count);
+    for (int i = 0; i < count; ++i)
+      fill[i] = offsets[i] - i;
+    for (size_t e = 0; e < edgesTotal; ++e) {
       const int i = (int)(std::upper_bound(offsets.begin(), offsets.end(), (long long)u[e]) -
                           offsets.begin()) - 1;
-      iu[i].push_back(u[e] - (int)offsets[i]);
-      iv[i].push_back(v[e] - (int)offsets[i]);
-      iw[i].push_back(w[e]);
-    }
-    for (int i = 0; i < count && st.ok(); ++i) {
-      if ((int)iu[i].size() != sizes[i] - 1) {
-        st(kErrorDisconnected);
+      const long long at = fill[i]++;
+      if (at >= offsets[i + 1] - (i + 1)) {
+        st(kErrorDisconnected); // more edges than the instance's tree has
         break;
       }
-      treeFromOrderedMerges(iu[i], iv[i], iw[i], sizes[i], hostTrees + (offsets[i] - i) * 4);
+      lu[at] = u[e] - (int)offsets[i];
+      lv[at] = v[e] - (int)offsets[i];
+      lw[at] = w[e];
+    }
+    std::atomic<int> next{0};
+    auto worker = [&]() {
+      for (int i = next++; i < count; i = next++) {
+        const long long first = offsets[i] - i;
+        treeFromOrderedMerges(lu.data() + first, lv.data() + first, lw.data() + first, sizes[i],
+                              hostTrees + first * 4);
+      }
+    };
+    if (st.ok()) {
+      const int threads =
+          (int)std::max(1u, std::min(std::thread::hardware_concurrency(), (unsigned)count));
+      std::vector<std::thread> pool;
+      for (int t = 1; t < threads; ++t)
+        pool.emplace_back(worker);
+      worker();
+      for (auto &th : pool)
+        th.join();
     }
   }
   if (hostCore && st.ok()) {

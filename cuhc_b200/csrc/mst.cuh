@@ -33,6 +33,8 @@ int sortEdgesToHost(DeviceEdges &edges, int numEdges, cudaStream_t stream, std::
 // treeFromOrderedMerges (mst.cuh:204-228). Z receives (n-1) x 4 doubles.
 void treeFromOrderedMerges(const std::vector<int> &u, const std::vector<int> &v,
                            const std::vector<float> &w, int n, double *Z);
+// The same over plain arrays of n - 1 merges.
+void treeFromOrderedMerges(const int *u, const int *v, const float *w, int n, double *Z);
 
 // Whether merges can form a tree: n-1 merges, finite heights, each joining
 // two clusters not yet joined (mst.cuh:188-202).

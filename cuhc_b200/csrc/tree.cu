@@ -102,6 +102,10 @@ inline int findRoot(std::vector<int> &parent, int x) {
 
 void treeFromOrderedMerges(const std::vector<int> &u, const std::vector<int> &v,
                            const std::vector<float> &w, int n, double *Z) {
+  treeFromOrderedMerges(u.data(), v.data(), w.data(), n, Z);
+}
+
+void treeFromOrderedMerges(const int *u, const int *v, const float *w, int n, double *Z) {
   std::vector<int> parent(n), size(n, 1), id(n);
   std::iota(parent.begin(), parent.end(), 0);
   std::iota(id.begin(), id.end(), 0);
