@@ -195,6 +195,86 @@ def run_batch(args, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_tree_workload(args, local_rank):
+    """Single-linkage 4M x 16 (radius proposal off / on) or Ward 1M x 32 (RNN
+    rounds): device-resident time per tree through the C ABI."""
+    import torch  # noqa: PLC0415
+    sys.path.insert(0, HERE)
+    import cuhc_b200 as C  # noqa: PLC0415
+    from cuhc_b200 import _lib  # noqa: PLC0415
+    from cuhc_b200.train_radius import make_anisotropic_blobs  # noqa: PLC0415
+    lib = _lib.lib
+    if args.workload == "c4":
+        X = make_anisotropic_blobs(3, args.n or 4_000_000)
+        linkage_id, algorithm, label = 0, 1, "single linkage (Borůvka)"
+    else:
+        X = np.random.default_rng(2).standard_normal((args.n or 1_000_000, 32)).astype(np.float32)
+        linkage_id, algorithm, label = 3, 3, "Ward (RNN rounds)"
+    n, d = X.shape
+    dev = torch.from_numpy(X).cuda()
+    tree = np.empty((n - 1) * 4, np.float64)
+
+    def step():
+        _lib.check(lib.cuhc_linkage_device(ctypes.c_void_p(dev.data_ptr()), n, d, 0, 2.0,
+                                           linkage_id, algorithm,
+                                           tree.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+
+    def timed(k):
+        times = []
+        for _ in range(k):
+            torch.cuda.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            step()
+            e.record()
+            e.synchronize()
+            times.append(s.elapsed_time(e) / 1e3)
+        return float(np.mean(times))
+
+    results = {}
+    variants = [("screened", "auto", None)]
+    if args.workload == "c4":
+        variants.append(("screened + radius proposal", "auto", "model"))
+    variants.append(("plain fp32", "off", None))
+    reference_tree = None
+    with ClockSampler(local_rank) as clocks:
+        for name, screen, radius in variants:
+            _lib.set_screen(screen)
+            if radius:
+                meta = C.load_radius_model()
+            for _ in range(args.warmup):
+                step()
+            C.radius_stats()
+            t = timed(args.steps)
+            stats = C.radius_stats()
+            results[name] = {"s": round(t, 4)}
+            if radius:
+                results[name]["certified_share"] = round(
+                    stats["certified"] / max(1, stats["proposed"]), 4)
+                results[name]["model"] = f"trained on seeds {list(meta['seeds'])}, " \
+                                         f"n = {int(meta['n'])}, {int(meta['rows'])} rows"
+                C.set_radius_model(None)
+            if reference_tree is None:
+                reference_tree = tree.copy()
+            results[name]["identical_tree"] = bool(np.array_equal(tree, reference_tree))
+    _lib.set_screen("auto")
+    best = min(v["s"] for v in results.values())
+    line = {
+        "metric": f"{n:,} x {d} {label} tree time (s) on 1 B200, exact",
+        "value": results["screened"]["s"], "unit": "s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(results["screened"]["s"] * 1e3, 1),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": ("4M x 16: 50 Gaussian clusters (shared random covariance, "
+                                "eigenvalues log-uniform in [0.05, 5]) + 5% noise, seed 3")
+                   if args.workload == "c4" else "1M x 32 standard normal, seed 2",
+                   "n": n, "d": d, "best_s": best},
+        "variants": results,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle samples during the timed region."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -343,13 +423,15 @@ def main():
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=["ours", "reference"], default="ours")
     parser.add_argument("--no-cpu-baseline", action="store_true")
-    parser.add_argument("--workload", choices=["hdbscan", "batch"], default="hdbscan",
-                        help="hdbscan: the headline tree; batch: many small instances")
+    parser.add_argument("--workload", choices=["hdbscan", "batch", "c4", "ward"],
+                        default="hdbscan",
+                        help="hdbscan: the headline tree; batch: many small instances; c4: "
+                             "4M x 16 single linkage; ward: 1M x 32 Ward")
     parser.add_argument("--instances", type=int, default=4096,
                         help="instances of the batch workload")
     parser.add_argument("--no-plain", action="store_true",
                         help="skip the screening-off comparison step")
-    parser.add_argument("--n", type=int, default=N_POINTS,
+    parser.add_argument("--n", type=int, default=None,
                         help="points of the same recipe (smaller cases for profiling)")
     args = parser.parse_args()
 
@@ -363,6 +445,17 @@ def main():
     if world > 1:
         from datetime import timedelta  # noqa: PLC0415
         dist.init_process_group("nccl", timeout=timedelta(minutes=5))
+
+    if args.workload in ("c4", "ward"):
+        if rank == 0 and args.impl == "ours":
+            run_tree_workload(args, local_rank)
+        elif rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "the secondary workloads are "
+                              "measured against the reference in the headline arm only"}),
+                  flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     if args.workload == "batch":
         if rank == 0 and args.impl == "ours":
@@ -386,7 +479,7 @@ def main():
     sys.path.insert(0, HERE)
     from cuhc_b200 import _lib  # noqa: PLC0415
 
-    X = make_blobs_with_noise(n=args.n)
+    X = make_blobs_with_noise(n=args.n or N_POINTS)
     n, d = X.shape
     f32, f64 = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double)
     X_dev = torch.from_numpy(X).cuda()

@@ -8,9 +8,10 @@ A drop-in for the Python API of cuhc (scipy / scikit-learn semantics):
 from ._batch import batched_trees
 from ._distances import METRIC_IDS, pairwise_distances
 from ._linkage import LINKAGE_IDS, fcluster, linkage
+from ._radius import load_radius_model, radius_stats, set_radius_model
 
 __all__ = ["LINKAGE_IDS", "METRIC_IDS", "batched_trees", "fcluster", "linkage",
-           "pairwise_distances"]
+           "load_radius_model", "pairwise_distances", "radius_stats", "set_radius_model"]
 
 try:  # estimators need scikit-learn
     from ._estimators import AgglomerativeClustering  # noqa: F401

@@ -21,6 +21,8 @@
 #pragma once
 
 #include <algorithm>
+#include <random>
+#include <type_traits>
 
 #include "profiling.cuh"
 #include "mst.cuh"
@@ -152,7 +154,7 @@ static __global__ void relabel(int *__restrict__ comp, const int *__restrict__ p
 
 template <class Metric, class Weight>
 int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, bool prune,
-               DeviceEdges &edges, PassStats *stats, cudaStream_t stream) {
+               DeviceEdges &edges, PassStats *stats, cudaStream_t stream, RadiusLog *radiusLog) {
   using namespace boruvka_detail;
   const int n = index.n;
   StatusChain st;
@@ -216,6 +218,43 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
   int maxJumps = 1;
   while ((1 << maxJumps) < n)
     ++maxJumps;
+  // Radius proposal (single linkage, one instance, 16 features, a model
+  // loaded) or training-row logging: per-round features of every position.
+  const RadiusModel model = currentRadiusModel();
+  const bool plainWeight = std::is_same<Weight, PlainWeight>::value;
+  const bool useRadius = plainWeight && !radiusLog && model.params && index.d == kRadiusDims &&
+                         index.numInstances == 1;
+  const bool logRows = plainWeight && radiusLog && index.d == kRadiusDims &&
+                       index.numInstances == 1;
+  DeviceBuffer<float> features, prediction, radius, targets;
+  DeviceBuffer<int> compSize;
+  DeviceBuffer<unsigned long long> certified;
+  if (useRadius || logRows) {
+    CUHC_TRY(st, features.allocate((size_t)n * kRadiusFeatures, stream));
+    CUHC_TRY(st, compSize.allocate(n, stream));
+    CUHC_TRY(st, prediction.allocate(n, stream));
+    CUHC_TRY(st, radius.allocate(n, stream));
+    CUHC_TRY(st, targets.allocate(n, stream));
+    CUHC_TRY(st, certified.allocate(1, stream));
+    CUHC_TRY(st, cudaMemsetAsync(certified.get(), 0, sizeof(unsigned long long), stream));
+  }
+  auto enqueueFeatures = [&](int round) {
+    StatusChain fs;
+    CUHC_TRY(fs, cudaMemsetAsync(compSize.get(), 0, n * sizeof(int), stream));
+    radius_detail::componentSizes<<<blocks(n), 256, 0, stream>>>(comp.get(), index.order.get(), n,
+                                                                 compSize.get());
+    noteLaunch();
+    radius_detail::radiusFeatures<<<blocks(n), 256, 0, stream>>>(
+        index.tiled.get(), n, index.d, index.kc, index.tileFloats(), index.order.get(),
+        index.nodeLow.get(), index.nodeHigh.get(), comp.get(), compSize.get(), nearest.get(),
+        round, features.get());
+    noteLaunch();
+    CUHC_TRY(fs, cudaGetLastError());
+    return fs.code;
+  };
+  std::mt19937_64 logRng(radiusLog ? radiusLog->seed : 0);
+  unsigned long long proposedRows = 0;
+
   // One round, enqueued on the stream with no host work: counters[0] counts
   // every edge so far (edges are written at absolute slots), counters[1..2]
   // this round's roots and unjumped parents.
@@ -230,17 +269,61 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
     }
     CUHC_TRY(rs, cudaGetLastError());
     p.singletons = first;
+    p.radius = nullptr;
+    if (useRadius || logRows)
+      CUHC_TRY(rs, enqueueFeatures(rounds));
+    if (useRadius) {
+      CUHC_TRY(rs, mlpForward(model.params, features.get(), n, prediction.get(), stream));
+      radius_detail::radiusFromPrediction<<<blocks(n), 256, 0, stream>>>(
+          prediction.get(), index.order.get(), n, model.offset, radius.get());
+      noteLaunch();
+      p.radius = radius.get();
+      proposedRows += (unsigned long long)index.numPoints;
+    }
     {
       PassTimer timer(timed ? (screened ? kTimerScreenPass : kTimerNearestPass) : -1, stream);
       if (screened)
         CUHC_TRY(rs, (launchScreen<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
       else
         CUHC_TRY(rs, (launchPass<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
+      if (useRadius) {
+        // Certify; the rest search again with no cap while certified rows sit out.
+        radius_detail::certifyRows<<<blocks(n), 256, 0, stream>>>(
+            nearest.get(), index.order.get(), n, radius.get(), certified.get());
+        noteLaunch();
+        if (screened)
+          CUHC_TRY(rs, (launchScreen<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
+        else
+          CUHC_TRY(rs, (launchPass<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
+        p.radius = nullptr;
+      }
       if (timer.start) {
         unsigned long long tilesNow = 0;
         cudaMemcpyAsync(&tilesNow, tiles.get(), sizeof(tilesNow), cudaMemcpyDeviceToHost, stream);
         timer.finish(tilesNow - tilesSoFar);
         tilesSoFar = tilesNow;
+      }
+    }
+    if (logRows) {
+      radius_detail::radiusTargets<<<blocks(n), 256, 0, stream>>>(nearest.get(), index.order.get(),
+                                                                  n, targets.get());
+      noteLaunch();
+      std::vector<float> hf((size_t)n * kRadiusFeatures), ht(n);
+      CUHC_TRY(rs, cudaMemcpyAsync(hf.data(), features.get(), hf.size() * sizeof(float),
+                                   cudaMemcpyDeviceToHost, stream));
+      CUHC_TRY(rs, cudaMemcpyAsync(ht.data(), targets.get(), ht.size() * sizeof(float),
+                                   cudaMemcpyDeviceToHost, stream));
+      CUHC_TRY(rs, cudaStreamSynchronize(stream));
+      std::vector<int> rows;
+      for (int i = 0; i < n; ++i)
+        if (std::isfinite(ht[i]))
+          rows.push_back(i);
+      std::shuffle(rows.begin(), rows.end(), logRng);
+      rows.resize(std::min<size_t>(rows.size(), (size_t)radiusLog->maxRowsPerRound));
+      for (const int i : rows) {
+        radiusLog->features.insert(radiusLog->features.end(), hf.begin() + (size_t)i * kRadiusFeatures,
+                                   hf.begin() + (size_t)(i + 1) * kRadiusFeatures);
+        radiusLog->targets.push_back(ht[i]);
       }
     }
     CUHC_TRY(rs, cudaMemsetAsync(compKey.get(), 0xff, n * sizeof(unsigned long long), stream));
@@ -316,6 +399,13 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
       st(kErrorNonFinite);
       break;
     }
+  }
+  if (useRadius) {
+    unsigned long long certifiedRows = 0;
+    cudaMemcpyAsync(&certifiedRows, certified.get(), sizeof(certifiedRows), cudaMemcpyDeviceToHost,
+                    stream);
+    cudaStreamSynchronize(stream);
+    addRadiusStats(proposedRows, certifiedRows);
   }
   if (graphExec)
     cudaGraphExecDestroy(graphExec);

@@ -534,6 +534,43 @@ int cuhc_trees_batched_device(const float *devicePoints, const long long *offset
   return st.code;
 }
 
+// Training rows for the radius model: runs the single-linkage Borůvka rounds
+// of points (HOST, n x 16) exactly and keeps up to maxRowsPerRound random
+// rows per round (seeded) of (19 features, log nearest other-component
+// weight). Writes min(rows, capacity) rows; *rows receives the count found.
+int cuhc_radius_training_rows(const float *hostPoints, int n, int d, int maxRowsPerRound,
+                              unsigned long long seed, float *features, float *targets,
+                              long long capacity, long long *rows) {
+  if (n < 2 || d != kRadiusDims || maxRowsPerRound < 1 || capacity < 0)
+    return kErrorInvalidShape;
+  CallContext ctx;
+  StatusChain st;
+  st(ctx.status);
+  DeviceBuffer<float> points;
+  CUHC_TRY(st, points.allocate((size_t)n * d, ctx.stream));
+  CUHC_TRY(st, cudaMemcpyAsync(points.get(), hostPoints, points.bytes(), cudaMemcpyHostToDevice,
+                               ctx.stream));
+  RadiusLog log;
+  log.maxRowsPerRound = maxRowsPerRound;
+  log.seed = seed;
+  SpatialIndex index;
+  CUHC_TRY(st, index.build(points.get(), n, d, true, ctx.stream));
+  DeviceEdges edges;
+  PassStats stats;
+  EuclideanMetric m;
+  CUHC_TRY(st, (boruvkaMst<EuclideanMetric, PlainWeight>(index, m, PlainWeight{}, true, edges,
+                                                          &stats, ctx.stream, &log)));
+  const long long found = (long long)log.targets.size();
+  if (rows)
+    *rows = found;
+  const long long keep = std::min(found, capacity);
+  if (st.ok() && keep > 0) {
+    std::copy(log.features.begin(), log.features.begin() + keep * kRadiusFeatures, features);
+    std::copy(log.targets.begin(), log.targets.begin() + keep, targets);
+  }
+  return st.code;
+}
+
 int cuhc_set_pruning(int mode) {
   if (mode < kPruneAuto || mode > kPruneNever)
     return kErrorInvalidAlgorithm;

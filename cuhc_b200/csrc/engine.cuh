@@ -159,6 +159,10 @@ struct PassParams {
   unsigned long long *screenStats; // ScreenCounter sums (null: not counted)
   const int *rootOfTile;  // traversal root per row tile (null: node 0)
   const int *coreRank;    // knn-mode rank per position, 0 = core 0 (null: k for all)
+  // Nearest mode: per-position cap on the row threshold (a proposed radius);
+  // a negative value marks a row that is already settled: it neither
+  // searches nor writes. Null: no cap.
+  const float *radius;
 };
 
 // Lower bound of every distance between the row tile box (shared memory)

@@ -24,13 +24,12 @@ int pairwiseDistances(const float *A, int nA, const float *B, int nB, int d, con
 } // namespace cuhc
 
 #define CUHC_INSTANTIATE_METRIC(M)                                                                 \
-  template int cuhc::boruvkaMst<M, cuhc::PlainWeight>(cuhc::SpatialIndex &, const M &,             \
-                                                      const cuhc::PlainWeight &, bool,             \
-                                                      cuhc::DeviceEdges &, cuhc::PassStats *,      \
-                                                      cudaStream_t);                               \
+  template int cuhc::boruvkaMst<M, cuhc::PlainWeight>(                                             \
+      cuhc::SpatialIndex &, const M &, const cuhc::PlainWeight &, bool, cuhc::DeviceEdges &,       \
+      cuhc::PassStats *, cudaStream_t, cuhc::RadiusLog *);                                         \
   template int cuhc::boruvkaMst<M, cuhc::MutualReachWeight>(                                       \
       cuhc::SpatialIndex &, const M &, const cuhc::MutualReachWeight &, bool, cuhc::DeviceEdges &, \
-      cuhc::PassStats *, cudaStream_t);                                                            \
+      cuhc::PassStats *, cudaStream_t, cuhc::RadiusLog *);                                                            \
   template int cuhc::coreDistances<M>(cuhc::SpatialIndex &, const M &, int, bool, float *,         \
                                       cuhc::PassStats *, cudaStream_t, const int *);                            \
   template bool cuhc::screenable<M>(cuhc::SpatialIndex &, int);                                    \

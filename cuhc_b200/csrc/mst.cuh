@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "radius.cuh"
 #include "spatial.cuh"
 
 namespace cuhc {
@@ -45,7 +46,8 @@ bool mergesFormTree(const std::vector<int> &u, const std::vector<int> &v,
 // boruvka_*.cu). Fills edges with the n-1 MST edges (original indices).
 template <class Metric, class Weight>
 int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, bool prune,
-               DeviceEdges &edges, PassStats *stats, cudaStream_t stream);
+               DeviceEdges &edges, PassStats *stats, cudaStream_t stream,
+               RadiusLog *radiusLog = nullptr);
 
 // Exact core distances (k-th nearest, the point itself first) by position.
 template <class Metric>

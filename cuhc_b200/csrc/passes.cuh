@@ -91,8 +91,12 @@ __device__ __forceinline__ void refreshThresholds(const PassParams &p, const Met
           cb = min(cb, atomicMin(slot, floatBits(thr)));
         thr = fminf(thr, bitsFloat(cb));
       }
+      // A proposed radius caps the threshold after the component exchange
+      // (only real edge weights go into compBest); negative: settled row.
+      if (valid && p.radius)
+        thr = fminf(thr, p.radius[pos]);
       const float v = valid ? w.load(pos) : 0.0f;
-      if (valid && w.feasible(thr, v))
+      if (valid && thr >= 0.0f && w.feasible(thr, v))
         filter = m.filterBound(w.distBound(thr, v));
     }
     sh.rowFilter[tid] = filter;
@@ -569,7 +573,7 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
       if (kKnn) {
         const int rank = p.coreRank ? p.coreRank[pos] : p.k;
         p.core[pos] = rank > 0 ? lists[tid * p.k + rank - 1] : 0.0f;
-      } else {
+      } else if (!p.radius || p.radius[pos] >= 0.0f) {
         p.nearest[pos] = sh.rowBest[tid];
       }
     }

@@ -314,8 +314,13 @@ __global__ void __launch_bounds__(kThreads, 2)
           cb = min(cb, atomicMin(compSlot, floatBits(thr)));
         thr = fminf(thr, bitsFloat(cb));
       }
-      F = (myValid && w.feasible(thr, myVal)) ? m.filterBound(w.distBound(thr, myVal))
-                                              : -INFINITY;
+      // A proposed radius caps the threshold after the component exchange
+      // (only real edge weights go into compBest); negative: settled row.
+      if (myValid && p.radius)
+        thr = fminf(thr, p.radius[myPos]);
+      F = (myValid && thr >= 0.0f && w.feasible(thr, myVal))
+              ? m.filterBound(w.distBound(thr, myVal))
+              : -INFINITY;
     }
     return F == -INFINITY ? -INFINITY : thr;
   };
@@ -622,7 +627,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (kKnn) {
       const int rank = myValid ? (p.coreRank ? p.coreRank[myPos] : p.k) : 0;
       p.core[myPos] = rank > 0 ? lists[myRow * p.k + rank - 1] : 0.0f;
-    } else {
+    } else if (!p.radius || p.radius[myPos] >= 0.0f) {
       p.nearest[myPos] = rowBest;
     }
   }

@@ -127,6 +127,31 @@ int cuhc_trees_batched_device(const float *devicePoints, const long long *offset
                               int numFeatures, int metricId, float metricParam,
                               const int *minSamples, double *trees, float *core);
 
+/* ---- learned radius proposal (no counterpart in the reference) ----------
+ * Single-linkage Borůvka rounds over 16 features can cap each row's search at
+ * a radius proposed by a 19 -> 64 -> 64 -> 1 BF16 MLP (5,505 parameters:
+ * W1[19][64], b1[64], W2[64][64], b2[64], w3[64], b3), certify the rows whose
+ * best edge lies inside it and search the rest again: trees never change. */
+
+/* Loads the model (HOST params) with its calibration offset (radius =
+ * exp(prediction + offset)); params NULL switches the proposal off. */
+int cuhc_set_radius_model(const float *params, float offset);
+/* Rows proposed and rows certified since the last call (first `count`). */
+int cuhc_radius_stats(unsigned long long *out, int count);
+/* Up to maxRowsPerRound random rows per exact single-linkage round of points
+ * (HOST, n x 16): features [rows][19], targets (log nearest other-component
+ * weight); at most `capacity` rows written, *rows = rows found. */
+int cuhc_radius_training_rows(const float *points, int n, int numFeatures, int maxRowsPerRound,
+                              unsigned long long seed, float *features, float *targets,
+                              long long capacity, long long *rows);
+/* The MLP on HOST buffers: forward (x [count][19] -> out), gradient of the
+ * mean squared error (and the error), and Adam training in place. */
+int cuhc_mlp_forward(const float *params, const float *x, int count, float *out);
+int cuhc_mlp_gradient(const float *params, const float *x, const float *y, int count, float *grad,
+                      float *loss);
+int cuhc_mlp_train(const float *x, const float *y, int count, int epochs, int batch, float lr,
+                   unsigned long long seed, float *params, float *losses);
+
 /* Tensor-core screening of the all-pairs passes: 0 auto (on for euclidean and
  * sqeuclidean up to 32 features), 1 on where supported, 2 off. Results never
  * change; returns CUHC_ERROR_INVALID_ALGORITHM for other values. */
