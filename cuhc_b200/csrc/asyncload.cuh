@@ -92,16 +92,31 @@ __device__ __forceinline__ uint64_t globalTimerNs() {
 // will: the kernel records kErrorTimeout and leaves.
 constexpr uint64_t kWaitLimitNs = 1000000000ull;
 
-// Waits for the barrier's phase `phase` to complete; false if a second of
-// wall-clock time (or the iteration limit) ran out first.
+// try_wait that lets the hardware suspend the thread (issuing nothing) until
+// the phase completes or about `hintNs` nanoseconds pass.
+__device__ __forceinline__ bool mbarrierTryWaitSuspend(uint64_t *bar, uint32_t phase,
+                                                       uint32_t hintNs) {
+  uint32_t done;
+  asm volatile("{\n\t.reg .pred p;\n\t"
+               "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+               "selp.u32 %0, 1, 0, p;\n\t}"
+               : "=r"(done)
+               : "r"(smemAddress(bar)), "r"(phase), "r"(hintNs)
+               : "memory");
+  return done != 0;
+}
+
+// Waits for the barrier's phase `phase` to complete, suspended in between
+// (a waiting warp takes no issue slots from the warps doing the work); false
+// if a second of wall-clock time (or the iteration limit) ran out first.
 __device__ __forceinline__ bool mbarrierWait(uint64_t *bar, uint32_t phase) {
   if (mbarrierTryWait(bar, phase))
     return true;
   const uint64_t start = globalTimerNs();
   for (long long spins = 0; spins < kSpinLimit; ++spins) {
-    if (mbarrierTryWait(bar, phase))
+    if (mbarrierTryWaitSuspend(bar, phase, 100000u))
       return true;
-    if ((spins & 63) == 63 && globalTimerNs() - start > kWaitLimitNs)
+    if (globalTimerNs() - start > kWaitLimitNs)
       return false;
   }
   return false;

@@ -270,6 +270,10 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
     CUHC_TRY(rs, cudaGetLastError());
     p.singletons = first;
     p.radius = nullptr;
+    // Heaviest row tiles first: by the last pass's work (boxes before any).
+    CUHC_TRY(rs, index.orderTiles(!index.tileWorkValid));
+    p.tileOrder = index.tileOrder.get();
+    p.tileWork = index.tileWork.get();
     if (useRadius || logRows)
       CUHC_TRY(rs, enqueueFeatures(rounds));
     if (useRadius) {
@@ -326,6 +330,7 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
         radiusLog->targets.push_back(ht[i]);
       }
     }
+    index.tileWorkValid = true;
     CUHC_TRY(rs, cudaMemsetAsync(compKey.get(), 0xff, n * sizeof(unsigned long long), stream));
     CUHC_TRY(rs, cudaMemsetAsync(compV.get(), 0xff, n * sizeof(unsigned int), stream));
     CUHC_TRY(rs, cudaMemsetAsync(counters.get() + 1, 0, 2 * sizeof(int), stream));
@@ -461,6 +466,9 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
   p.core = core;
   p.k = k;
   p.coreRank = coreRank;
+  CUHC_TRY(st, index.orderTiles(!index.tileWorkValid));
+  p.tileOrder = index.tileOrder.get();
+  p.tileWork = index.tileWork.get();
   p.tilesComputed = tiles.get();
   p.error = error.get();
   p.screenStats = screenCounters();
@@ -481,6 +489,7 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
       timer.finish(tilesNow);
     }
   }
+  index.tileWorkValid = true;
   int err = 0;
   unsigned long long tileCount = 0;
   CUHC_TRY(st, cudaMemcpyAsync(&err, error.get(), sizeof(int), cudaMemcpyDeviceToHost, stream));

@@ -163,6 +163,11 @@ struct PassParams {
   // a negative value marks a row that is already settled: it neither
   // searches nor writes. Null: no cap.
   const float *radius;
+  // Block b takes row tile tileOrder[b] (null: b), so that the heaviest row
+  // tiles start first; tileWork[I] receives the column tiles row tile I
+  // computed (null: not recorded).
+  const int *tileOrder;
+  unsigned int *tileWork;
 };
 
 // Lower bound of every distance between the row tile box (shared memory)

@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
 
   const TileGeom g;
   const int tid = threadIdx.x;
-  const int I = blockIdx.x;
+  const int I = p.tileOrder ? p.tileOrder[blockIdx.x] : (int)blockIdx.x;
   const int firstRow = I * kTile;
   const int leaf = p.leafOfTile[I];
   const int rowPure = (!kKnn && p.nodePure) ? p.nodePure[leaf] : -1;
@@ -579,6 +579,8 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
     }
   }
   if (tid == 0) {
+    if (p.tileWork)
+      p.tileWork[I] = (unsigned int)computed;
     if (p.tilesComputed)
       atomicAdd(p.tilesComputed, computed);
     if (failed && p.error)

@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool consumer = tid < kTile;
   const bool control = tid == kControlWarp * 32;
-  const int I = blockIdx.x;
+  const int I = p.tileOrder ? p.tileOrder[blockIdx.x] : (int)blockIdx.x;
   const int firstRow = I * kTile;
   const int leaf = p.leafOfTile[I];
   const int rowPure = (!kKnn && p.nodePure) ? p.nodePure[leaf] : -1;
@@ -648,6 +648,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     tmemDealloc(tmem, 256);
   }
   if (tid == 0) {
+    if (p.tileWork)
+      p.tileWork[I] = (unsigned int)computed;
     if (p.tilesComputed)
       atomicAdd(p.tilesComputed, computed);
     if (p.screenStats && maskPass)

@@ -538,6 +538,64 @@ bool SpatialIndex::extentsWithin(float limit) {
   return true;
 }
 
+namespace {
+
+__global__ void tileKeysFromBoxes(const float *__restrict__ low, const float *__restrict__ high,
+                                  const int *__restrict__ leafOfTile, int d, int numTiles,
+                                  unsigned int *__restrict__ keys, int *__restrict__ iota) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= numTiles)
+    return;
+  const int node = leafOfTile[t];
+  float score = 0.0f;
+  for (int f = 0; f < d; ++f)
+    score += __log2f(fmaxf(high[(size_t)node * d + f] - low[(size_t)node * d + f], 1e-30f));
+  keys[t] = orderedBits(score);
+  iota[t] = t;
+}
+
+__global__ void tileKeysFromWork(const unsigned int *__restrict__ work, int numTiles,
+                                 unsigned int *__restrict__ keys, int *__restrict__ iota) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= numTiles)
+    return;
+  keys[t] = work[t];
+  iota[t] = t;
+}
+
+} // namespace
+
+int SpatialIndex::orderTiles(bool fromBoxes) {
+  StatusChain st;
+  if (!tileOrder.get()) {
+    CUHC_TRY(st, tileWork.allocate(numTiles, stream));
+    CUHC_TRY(st, tileOrder.allocate(numTiles, stream));
+    CUHC_TRY(st, tileKeys.allocate(numTiles, stream));
+    CUHC_TRY(st, tileKeysSorted.allocate(numTiles, stream));
+    CUHC_TRY(st, tileIota.allocate(numTiles, stream));
+    CUHC_TRY(st, cub::DeviceRadixSort::SortPairsDescending(
+                     nullptr, tileSortBytes, tileKeys.get(), tileKeysSorted.get(), tileIota.get(),
+                     tileOrder.get(), numTiles, 0, 32, stream));
+    CUHC_TRY(st, tileSortTemp.allocate(std::max<size_t>(tileSortBytes, 1), stream));
+    CUHC_TRY(st, cudaMemsetAsync(tileWork.get(), 0, numTiles * sizeof(unsigned int), stream));
+    if (!st.ok())
+      return st.code;
+  }
+  if (fromBoxes)
+    tileKeysFromBoxes<<<blocksFor(numTiles, 256), 256, 0, stream>>>(
+        nodeLow.get(), nodeHigh.get(), leafOfTile.get(), d, numTiles, tileKeys.get(),
+        tileIota.get());
+  else
+    tileKeysFromWork<<<blocksFor(numTiles, 256), 256, 0, stream>>>(
+        tileWork.get(), numTiles, tileKeys.get(), tileIota.get());
+  noteLaunch();
+  CUHC_TRY(st, cudaGetLastError());
+  CUHC_TRY(st, cub::DeviceRadixSort::SortPairsDescending(
+                   tileSortTemp.get(), tileSortBytes, tileKeys.get(), tileKeysSorted.get(),
+                   tileIota.get(), tileOrder.get(), numTiles, 0, 32, stream));
+  return st.code;
+}
+
 int SpatialIndex::updatePurity(const int *component) {
   leafSummaryKernel<<<blocksFor((long long)numTiles * 32, 128), 128, 0, stream>>>(
       n, numTiles, leafOfTile.get(), nullptr, component, nullptr, nodePure.get()); noteLaunch();

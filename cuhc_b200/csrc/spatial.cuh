@@ -59,6 +59,14 @@ struct SpatialIndex {
   std::vector<int> instanceFirstTile;    // host, per instance
   DeviceBuffer<int> rootOfTile;          // traversal root per tile (batches)
   DeviceBuffer<unsigned char> nodeSpans; // batches
+  // Heavy-first launch order of the passes (orderTiles).
+  DeviceBuffer<unsigned int> tileWork;   // column tiles each row tile computed last pass
+  DeviceBuffer<int> tileOrder;           // row tiles, heaviest first
+  DeviceBuffer<unsigned int> tileKeys, tileKeysSorted;
+  DeviceBuffer<int> tileIota;
+  DeviceBuffer<unsigned char> tileSortTemp;
+  size_t tileSortBytes = 0;
+  bool tileWorkValid = false;            // a pass has recorded tileWork
 
   size_t tileFloats() const { return (size_t)numChunks * kc * kTile; }
 
@@ -83,6 +91,10 @@ struct SpatialIndex {
   // finite and at most `limit`. Copies the root box to the host and waits
   // for the index stream.
   bool extentsWithin(float limit);
+  // tileOrder <- row tiles by decreasing tileWork (fromBoxes: by decreasing
+  // leaf box log-volume, the estimate before any pass has run). Enqueued on
+  // the index stream with no host work (buffers are allocated on first use).
+  int orderTiles(bool fromBoxes);
 };
 
 } // namespace cuhc
