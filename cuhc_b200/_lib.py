@@ -104,16 +104,16 @@ def set_screen(mode):
     check(lib.cuhc_set_screen(SCREEN_MODES[mode]))
 
 
-SCREEN_COUNTERS = ("rechecks", "slow_rows", "indicator_tiles", "masked_tiles")
+SCREEN_COUNTERS = ("rechecks", "slow_rows", "indicator_tiles", "masked_tiles", "prefiltered")
 
 
 def screen_counters():
     """Screened-pass counters since the last call (counted while timing is
     on): exact rechecks, row visits that took the exact path, tiles whose
     components were excluded by indicator slots, tiles masked in the
-    epilogue."""
-    out = (ctypes.c_uint64 * 4)()
-    check(lib.cuhc_screen_counters(out, 4))
+    epilogue, candidate tiles no row of the block needed."""
+    out = (ctypes.c_uint64 * len(SCREEN_COUNTERS))()
+    check(lib.cuhc_screen_counters(out, len(SCREEN_COUNTERS)))
     return dict(zip(SCREEN_COUNTERS, (int(x) for x in out)))
 
 

@@ -84,7 +84,7 @@ int cuhc_kernel_timing(double *ms, unsigned long long *launches, unsigned long l
 
 // Screened-pass counters of the current device since the last call (first
 // `count` of: exact rechecks, exact-path row visits, indicator tiles, masked
-// tiles); resets them. Counted only while timing is on.
+// tiles, tiles no row needed); resets them. Counted only while timing is on.
 int cuhc_screen_counters(unsigned long long *out, int count) {
   unsigned long long host[cuhc::kNumScreenCounters] = {};
   cudaError_t e = cudaMemcpyFromSymbol(host, cuhc::gScreenCounterArray, sizeof(host));

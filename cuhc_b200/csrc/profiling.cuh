@@ -21,9 +21,11 @@ bool timingEnabled();
 // Screened-pass counters (device memory of the current device), summed by
 // the screened kernels while timing is on: exact rechecks, row visits that
 // took the exact path, tiles whose components were excluded by indicator
-// slots, tiles masked by component in the epilogue.
+// slots, tiles masked by component in the epilogue, candidate tiles that no
+// row of the block needed (skipped before any copy).
 enum ScreenCounter : int { kScreenRechecks = 0, kScreenSlowRows = 1, kScreenIndicatorTiles = 2,
-                           kScreenMaskedTiles = 3, kNumScreenCounters = 4 };
+                           kScreenMaskedTiles = 3, kScreenPrefiltered = 4,
+                           kNumScreenCounters = 5 };
 // Null when timing is off (the kernels then count nothing).
 unsigned long long *screenCounters();
 

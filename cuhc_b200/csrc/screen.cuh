@@ -64,6 +64,7 @@ constexpr int kScreenMaxSlots = 8;
 constexpr int kBuilderWarps = 3; // warps 4..6 build column operands
 constexpr int kBuilderThreads = 32 * kBuilderWarps;
 constexpr int kControlWarp = 7;  // issues the bulk copies and the MMAs
+constexpr int kFirstPhase = 16;  // tiles of a batch's first phase (then x4 per phase)
 constexpr float kIndicator = 0x1p90f;
 constexpr float kScreenAbsSlack = 0x1p-70f;
 constexpr float kScreenMaxExtent = 0x1p40f;
@@ -100,6 +101,8 @@ struct ScreenSync {
   int rawTile[kScreenStages]; // column tile (| kPureColumnTile) per ring slot, -1 ends the batch
   int slotTile[2];            // the same, per accumulator
   float warpThr[4];
+  float rowF[kTile]; // each row's filter bound as last refreshed (-inf: gains nothing)
+  int cursor, batchDone; // the control's place in the candidate list at a phase end
   int rowSet[kScreenMaxSlots];
   int rowSetCount, oneHot, failed;
   uint32_t tmemBase;
@@ -333,6 +336,8 @@ __global__ void __launch_bounds__(kThreads, 2)
   };
   if (consumer)
     warpMaxThr(refresh(compSlot ? __ldcg(compSlot) : 0xffffffffu));
+  if (consumer)
+    ss.rowF[myRow] = F;
   __syncthreads();
   if (tid == 0)
     sh.thrTile = fmaxf(fmaxf(ss.warpThr[0], ss.warpThr[1]), fmaxf(ss.warpThr[2], ss.warpThr[3]));
@@ -345,12 +350,46 @@ __global__ void __launch_bounds__(kThreads, 2)
   int t = 0;      // ordinal of tiles and sentinels through the rings (all threads agree)
   int issued = 0; // control: ordinals issued
   int lastCommit = -1;
+  unsigned long long prefiltered = 0; // candidate tiles no row needed (per thread)
   unsigned long long computed = 0;
   bool selfPending = kKnn || rowPure < 0;
   bool overflow = false;
   bool dirty = false;                          // consumer: row filter may have tightened
   unsigned long long rechecks = 0, slowRows = 0; // consumer counters
 
+  const float pruneScale = (1.0f - boxSlack(p.d)) * (1.0f - boxSlack(p.d));
+  // Whether any row of the tile can still gain from column tile `entry`:
+  // its point-to-box squared lower bound (scaled by the box slack) at most
+  // the row's published filter bound. One thread per candidate: the box in
+  // registers (features past d are zero on both sides and add nothing), rows
+  // and bounds read as shared-memory broadcasts, stopping at the first row
+  // that needs the tile.
+  auto rowsNeed = [&](int entry) -> bool {
+    const int leafJ = p.leafOfTile[entry & ~kPureColumnTile];
+    const float *lo = p.nodeLow + (size_t)leafJ * p.d, *hi = p.nodeHigh + (size_t)leafJ * p.d;
+    float blo[KC], bhi[KC];
+#pragma unroll
+    for (int k = 0; k < KC; ++k) {
+      blo[k] = k < p.d ? __ldg(lo + k) : 0.0f;
+      bhi[k] = k < p.d ? __ldg(hi + k) : 0.0f;
+    }
+    for (int r = 0; r < kTile; ++r) {
+      const float F = ((volatile float *)ss.rowF)[r];
+      if (!(F >= 0.0f))
+        continue; // a row that gains nothing
+      float s2 = 0.0f;
+#pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        const float x = sA[k * kTile + r];
+        const float g = fmaxf(0.0f, fmaxf(blo[k] - x, x - bhi[k]));
+        s2 = fmaf(g, g, s2);
+      }
+      if (s2 * pruneScale <= F)
+        return true;
+    }
+    return false;
+  };
+  int batch = 0;
   while (true) {
     if (warp == 0)
       collectCandidates(p, m, w, sh, rowLow, rowHigh, I, rowPure, rowMinValue, slack);
@@ -366,32 +405,49 @@ __global__ void __launch_bounds__(kThreads, 2)
       sortCandidates(sh, len);
     __syncthreads();
 
+    // Phases of the batch: the control issues phaseLimit tiles (kFirstPhase,
+    // then four times more each phase) and a sentinel; between phases every
+    // warp tests the remaining candidates against the rows' current bounds.
+    int cursor = 0, phaseLimit = kFirstPhase;
+    for (int phase = 0;; ++phase) {
+    if (p.prune && (batch > 0 || phase > 0)) {
+      for (int c = cursor + tid; c < len; c += kThreads)
+        if (sh.listLb[c] < INFINITY && !rowsNeed(sh.listTile[c])) {
+          sh.listLb[c] = INFINITY;
+          ++prefiltered;
+        }
+      __syncthreads();
+    }
+
     if (warp == kControlWarp) {
-      // ---- control: bulk copies and MMAs (lane 0) ----
-      if (lane == 0) {
-        int cursor = 0;
-        bool sentinelIssued = false;
-        // Issues ordinal `issued` into its ring slot: a column tile, or the
-        // batch's sentinel. The slot's previous ordinal (issued - stages) is
-        // done with: at a batch start every ordinal is, and later the caller
-        // has seen every consumer warp release ordinal issued - kScreenAhead
-        // - 2, which each of them does after finishing issued - stages.
-        auto issueNext = [&]() {
-          const int r = issued % kScreenStages;
-          int entry = -1;
-          if (selfPending) {
-            entry = I;
-            selfPending = false;
-          } else {
-            const float thr = *(volatile float *)&sh.thrTile;
-            while (cursor < len && sh.listLb[cursor] > thr)
-              ++cursor;
-            if (cursor < len)
-              entry = sh.listTile[cursor++];
-          }
+      // ---- control: lane 0 issues the bulk copies and the MMAs; the whole
+      // warp runs the loop in step and tests candidate tiles row by row ----
+      bool sentinelIssued = false;
+      int phaseIssued = 0;
+      // Issues ordinal `issued` into its ring slot: a column tile, or the
+      // batch's sentinel. The slot's previous ordinal (issued - stages) is
+      // done with: at a batch start every ordinal is, and later the caller
+      // has seen every consumer warp release ordinal issued - kScreenAhead
+      // - 2, which each of them does after finishing issued - stages.
+      auto issueNext = [&]() {
+        const int r = issued % kScreenStages;
+        int entry = -1;
+        if (selfPending) {
+          entry = I;
+          selfPending = false;
+        } else if (phaseIssued < phaseLimit) {
+          const float thr =
+              __shfl_sync(0xffffffffu, lane == 0 ? *(volatile float *)&sh.thrTile : 0.0f, 0);
+          while (cursor < len && sh.listLb[cursor] > thr)
+            ++cursor;
+          if (cursor < len)
+            entry = sh.listTile[cursor++];
+        }
+        if (entry >= 0)
+          ++phaseIssued;
+        if (lane == 0) {
           ss.rawTile[r] = entry;
           if (entry < 0) {
-            sentinelIssued = true;
             mbarrierArrive(&ss.rawFull[r], 1);
           } else {
             const int J = entry & ~kPureColumnTile;
@@ -408,21 +464,28 @@ __global__ void __launch_bounds__(kThreads, 2)
               bulkCopyToShared(meta + 2 * kTile, w.value + (size_t)J * kTile,
                                kTile * sizeof(float), &ss.rawFull[r]);
           }
-          ++issued;
-        };
-        while (!sentinelIssued && issued <= t + kScreenAhead)
-          issueNext();
-        while (true) {
-          const int s = t & 1;
-          // Every consumer warp released ordinal t - 2: accumulator s is
-          // free, and so is the ring slot of ordinal t + kScreenAhead.
-          bool ok = screenWait(&ss.tmemEmpty[s], ((t >> 1) & 1) ^ 1, ss);
-          if (ok)
-            while (!sentinelIssued && issued <= t + kScreenAhead)
-              issueNext();
-          const int entry = ss.rawTile[t % kScreenStages];
-          // The builders finished the column operand of ordinal t.
-          ok = ok && entry >= 0 && screenWait(&ss.opBReady[s], (t >> 1) & 1, ss);
+        }
+        if (entry < 0)
+          sentinelIssued = true;
+        ++issued;
+      };
+      while (!sentinelIssued && issued <= t + kScreenAhead)
+        issueNext();
+      while (true) {
+        const int s = t & 1;
+        // Every consumer warp released ordinal t - 2: accumulator s is free,
+        // and so is the ring slot of ordinal t + kScreenAhead.
+        bool ok = __shfl_sync(0xffffffffu, screenWait(&ss.tmemEmpty[s], ((t >> 1) & 1) ^ 1, ss), 0);
+        if (ok)
+          while (!sentinelIssued && issued <= t + kScreenAhead)
+            issueNext();
+        __syncwarp();
+        const int entry = ss.rawTile[t % kScreenStages];
+        // The builders finished the column operand of ordinal t.
+        if (ok && entry >= 0)
+          ok = screenWait(&ss.opBReady[s], (t >> 1) & 1, ss);
+        ok = __shfl_sync(0xffffffffu, ok && entry >= 0, 0);
+        if (lane == 0) {
           if (ok) {
             tcgenFenceAfter();
             const float *b = opB + (size_t)s * kTile * kPad;
@@ -438,12 +501,11 @@ __global__ void __launch_bounds__(kThreads, 2)
             ss.slotTile[s] = -1; // the batch's end (or a failed wait) goes on to the consumers
             mbarrierArrive(&ss.mmaFull[s], 2);
           }
-          ++t;
-          if (!ok)
-            break;
         }
+        ++t;
+        if (!ok)
+          break;
       }
-      t = __shfl_sync(0xffffffffu, t, 0);
     } else if (!consumer) {
       // ---- builders: warps 4..6, column j and (warp 4) column j + 96 ----
       const int j = tid - kTile;
@@ -586,6 +648,7 @@ __global__ void __launch_bounds__(kThreads, 2)
           // eighth tile for the latter.
           if (__any_sync(0xffffffffu, dirty) || (computed & 7) == 7) {
             warpMaxThr(refresh(compSlot ? __ldcg(compSlot) : 0xffffffffu));
+            ss.rowF[myRow] = F; // published for the control warp's row test
             dirty = false;
             thrChanged = true;
           }
@@ -605,10 +668,20 @@ __global__ void __launch_bounds__(kThreads, 2)
           break;
       }
     }
+    if (warp == kControlWarp && lane == 0) {
+      ss.cursor = cursor;
+      ss.batchDone = cursor >= len ? 1 : 0;
+    }
     __syncthreads();
-    // The control issued the row tile itself first in the first batch; every
+    // The control issued the row tile itself first in the first phase; every
     // thread forgets it here so that the loop's exit stays uniform.
     selfPending = false;
+    cursor = ss.cursor;
+    if (ss.failed || ss.batchDone)
+      break;
+    phaseLimit *= 4;
+    } // phases
+    ++batch;
     if (ss.failed)
       break;
     if (sh.frontLen == 0)
@@ -640,6 +713,12 @@ __global__ void __launch_bounds__(kThreads, 2)
       atomicAdd(p.screenStats + kScreenRechecks, rechecks);
       atomicAdd(p.screenStats + kScreenSlowRows, slowRows);
     }
+  }
+  if (p.screenStats) {
+    for (int off = 16; off > 0; off /= 2)
+      prefiltered += __shfl_xor_sync(0xffffffffu, prefiltered, off);
+    if (lane == 0 && prefiltered)
+      atomicAdd(p.screenStats + kScreenPrefiltered, prefiltered);
   }
   tcgenFenceBefore();
   __syncthreads();

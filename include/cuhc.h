@@ -190,7 +190,8 @@ int cuhc_kernel_timing(double *ms, unsigned long long *launches, unsigned long l
 /* Screened-pass counters since the last call, summed while timing is on
  * (first `count` of): exact FP32 rechecks, row visits that took the exact
  * path, tiles whose components were excluded by indicator slots, tiles
- * masked by component in the epilogue. Resets them. */
+ * masked by component in the epilogue, candidate tiles that no row of their
+ * block needed. Resets them. */
 int cuhc_screen_counters(unsigned long long *out, int count);
 
 #ifdef __cplusplus
