@@ -64,7 +64,7 @@ constexpr int kScreenMaxSlots = 8;
 constexpr int kBuilderWarps = 3; // warps 4..6 build column operands
 constexpr int kBuilderThreads = 32 * kBuilderWarps;
 constexpr int kControlWarp = 7;  // issues the bulk copies and the MMAs
-constexpr int kFirstPhase = 16;  // tiles of a batch's first phase (then x4 per phase)
+constexpr int kFirstPhase = 64;  // tiles of a batch's first phase (then x8 per phase)
 constexpr float kIndicator = 0x1p90f;
 constexpr float kScreenAbsSlack = 0x1p-70f;
 constexpr float kScreenMaxExtent = 0x1p40f;
@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     __syncthreads();
 
     // Phases of the batch: the control issues phaseLimit tiles (kFirstPhase,
-    // then four times more each phase) and a sentinel; between phases every
+    // then eight times more each phase) and a sentinel; between phases every
     // warp tests the remaining candidates against the rows' current bounds.
     int cursor = 0, phaseLimit = kFirstPhase;
     for (int phase = 0;; ++phase) {
@@ -679,7 +679,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     cursor = ss.cursor;
     if (ss.failed || ss.batchDone)
       break;
-    phaseLimit *= 4;
+    phaseLimit *= 8;
     } // phases
     ++batch;
     if (ss.failed)
