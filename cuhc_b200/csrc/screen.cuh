@@ -102,6 +102,7 @@ struct ScreenSync {
   int slotTile[2];            // the same, per accumulator
   float warpThr[4];
   float rowF[kTile]; // each row's filter bound as last refreshed (-inf: gains nothing)
+  float groupF[4];   // the largest rowF of each consumer warp's 32 rows
   int cursor, batchDone; // the control's place in the candidate list at a phase end
   int rowSet[kScreenMaxSlots];
   int rowSetCount, oneHot, failed;
@@ -199,6 +200,8 @@ __global__ void __launch_bounds__(kThreads, 2)
   extern __shared__ __align__(128) float dyn[];
   __shared__ PassState sh;
   __shared__ ScreenSync ss;
+  // Bounding box of each consumer warp's valid rows (+inf/-inf when none).
+  __shared__ float groupLow[4 * KC], groupHigh[4 * KC];
   float *sA = dyn + L::sA;
   float *rawBase = dyn + L::raw;
   int *metaBase = reinterpret_cast<int *>(dyn + L::meta);
@@ -297,8 +300,23 @@ __global__ void __launch_bounds__(kThreads, 2)
   tcgenFenceAfter();
   const uint32_t tmem = ss.tmemBase;
   const bool oneHot = ss.oneHot != 0;
-  if (consumer)
+  if (consumer) {
     buildRowOperand<KC>(sA, centre, scale, myRow, myValid, myComp, ss, opA);
+#pragma unroll
+    for (int k = 0; k < KC; ++k) {
+      float lo = myValid ? sA[k * kTile + myRow] : INFINITY;
+      float hi = myValid ? sA[k * kTile + myRow] : -INFINITY;
+#pragma unroll
+      for (int off = 16; off > 0; off /= 2) {
+        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, off));
+        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, off));
+      }
+      if (lane == 0) {
+        groupLow[warp * KC + k] = lo;
+        groupHigh[warp * KC + k] = hi;
+      }
+    }
+  }
   fenceProxyAsync();
 
   // Row threshold: sets F (the row's filter bound) and returns the row's
@@ -327,17 +345,23 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
     return F == -INFINITY ? -INFINITY : thr;
   };
-  auto warpMaxThr = [&](float t) {
+  // Publishes the warp's largest threshold (for the block's candidate cut),
+  // each row's F and the warp's largest F (for the tile tests).
+  auto publish = [&](float t) {
+    float f = F;
 #pragma unroll
-    for (int off = 16; off > 0; off /= 2)
+    for (int off = 16; off > 0; off /= 2) {
       t = fmaxf(t, __shfl_xor_sync(0xffffffffu, t, off));
-    if (lane == 0)
+      f = fmaxf(f, __shfl_xor_sync(0xffffffffu, f, off));
+    }
+    ss.rowF[myRow] = F;
+    if (lane == 0) {
       ss.warpThr[warp] = t;
+      ss.groupF[warp] = f;
+    }
   };
   if (consumer)
-    warpMaxThr(refresh(compSlot ? __ldcg(compSlot) : 0xffffffffu));
-  if (consumer)
-    ss.rowF[myRow] = F;
+    publish(refresh(compSlot ? __ldcg(compSlot) : 0xffffffffu));
   __syncthreads();
   if (tid == 0)
     sh.thrTile = fmaxf(fmaxf(ss.warpThr[0], ss.warpThr[1]), fmaxf(ss.warpThr[2], ss.warpThr[3]));
@@ -363,7 +387,10 @@ __global__ void __launch_bounds__(kThreads, 2)
   // the row's published filter bound. One thread per candidate: the box in
   // registers (features past d are zero on both sides and add nothing), rows
   // and bounds read as shared-memory broadcasts, stopping at the first row
-  // that needs the tile.
+  // that needs the tile. Each warp's 32 rows are first tested as a group:
+  // the box-to-box bound against the group's largest F. Rounding is
+  // monotone, so the group bound never exceeds any member row's bound and
+  // a group that fails holds no row that passes.
   auto rowsNeed = [&](int entry) -> bool {
     const int leafJ = p.leafOfTile[entry & ~kPureColumnTile];
     const float *lo = p.nodeLow + (size_t)leafJ * p.d, *hi = p.nodeHigh + (size_t)leafJ * p.d;
@@ -373,19 +400,33 @@ __global__ void __launch_bounds__(kThreads, 2)
       blo[k] = k < p.d ? __ldg(lo + k) : 0.0f;
       bhi[k] = k < p.d ? __ldg(hi + k) : 0.0f;
     }
-    for (int r = 0; r < kTile; ++r) {
-      const float F = ((volatile float *)ss.rowF)[r];
-      if (!(F >= 0.0f))
-        continue; // a row that gains nothing
-      float s2 = 0.0f;
+    for (int g = 0; g < 4; ++g) {
+      const float gF = ((volatile float *)ss.groupF)[g];
+      if (!(gF >= 0.0f))
+        continue; // no row of the group gains anything
+      float b2 = 0.0f;
 #pragma unroll
       for (int k = 0; k < KC; ++k) {
-        const float x = sA[k * kTile + r];
-        const float g = fmaxf(0.0f, fmaxf(blo[k] - x, x - bhi[k]));
-        s2 = fmaf(g, g, s2);
+        const float gap = fmaxf(0.0f, fmaxf(blo[k] - groupHigh[g * KC + k],
+                                            groupLow[g * KC + k] - bhi[k]));
+        b2 = fmaf(gap, gap, b2);
       }
-      if (s2 * pruneScale <= F)
-        return true;
+      if (b2 * pruneScale > gF)
+        continue;
+      for (int r = 32 * g; r < 32 * g + 32; ++r) {
+        const float F = ((volatile float *)ss.rowF)[r];
+        if (!(F >= 0.0f))
+          continue; // a row that gains nothing
+        float s2 = 0.0f;
+#pragma unroll
+        for (int k = 0; k < KC; ++k) {
+          const float x = sA[k * kTile + r];
+          const float gap = fmaxf(0.0f, fmaxf(blo[k] - x, x - bhi[k]));
+          s2 = fmaf(gap, gap, s2);
+        }
+        if (s2 * pruneScale <= F)
+          return true;
+      }
     }
     return false;
   };
@@ -647,8 +688,7 @@ __global__ void __launch_bounds__(kThreads, 2)
           // component's best (found by other blocks): refresh then, and every
           // eighth tile for the latter.
           if (__any_sync(0xffffffffu, dirty) || (computed & 7) == 7) {
-            warpMaxThr(refresh(compSlot ? __ldcg(compSlot) : 0xffffffffu));
-            ss.rowF[myRow] = F; // published for the control warp's row test
+            publish(refresh(compSlot ? __ldcg(compSlot) : 0xffffffffu));
             dirty = false;
             thrChanged = true;
           }
