@@ -186,12 +186,27 @@ __device__ __forceinline__ void nearestEpilogue(const Metric &m, const Weight &w
 __device__ __forceinline__ void insertSorted(float *list, int k, float v) {
   if (!(v < list[k - 1]))
     return;
-  int pos = k - 1;
-  while (pos > 0 && list[pos - 1] > v) {
-    list[pos] = list[pos - 1];
-    --pos;
+  // Place: after every entry <= v (binary search; list[k - 1] > v), then the
+  // tail moves up one slot, four independent loads before their stores.
+  int lo = 0, hi = k - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (list[mid] > v)
+      hi = mid;
+    else
+      lo = mid + 1;
   }
-  list[pos] = v;
+  int i = k - 1;
+  for (; i - 4 >= lo; i -= 4) {
+    const float a = list[i - 1], b = list[i - 2], c = list[i - 3], d = list[i - 4];
+    list[i] = a;
+    list[i - 1] = b;
+    list[i - 2] = c;
+    list[i - 3] = d;
+  }
+  for (; i > lo; --i)
+    list[i] = list[i - 1];
+  list[lo] = v;
 }
 
 template <class Metric>
@@ -270,23 +285,30 @@ __device__ void collectCandidates(const PassParams &p, const Metric &m, const We
     bool keepLeaf = false, expand = false;
     int tile = -1;
     float lb = 0.0f;
+    int left = -1, right = -1;
     if (node >= 0) {
-      const int pure = p.nodePure ? p.nodePure[node] : -1;
+      // Every field of the node is loaded before any is used: one round
+      // trip to L2 per step of the walk.
+      const int pure = p.nodePure ? __ldg(p.nodePure + node) : -1;
+      left = __ldg(p.nodeLeft + node);
+      right = __ldg(p.nodeRight + node);
+      const int first = __ldg(p.nodeFirstTile + node);
+      const float v = p.nodeMinValue ? __ldg(p.nodeMinValue + node) : 0.0f;
       const bool skip = rowPure >= 0 && pure == rowPure;
       if (!skip && p.prune && Metric::kBoxBound) {
         typename Metric::Acc acc = m.init();
         const float *lo = p.nodeLow + (size_t)node * p.d, *hi = p.nodeHigh + (size_t)node * p.d;
+#pragma unroll 8
         for (int f = 0; f < p.d; ++f) {
           const float gap =
               fmaxf(0.0f, fmaxf(__ldg(lo + f) - rowHigh[f], rowLow[f] - __ldg(hi + f)));
           acc = m.accumulate(acc, gap, 0.0f);
         }
-        const float v = p.nodeMinValue ? p.nodeMinValue[node] : 0.0f;
         lb = w.lowerBound(m.finalize(acc), rowMinValue, v) * slack;
       }
       if (!skip && lb <= thr) {
-        if (p.nodeLeft[node] < 0) {
-          tile = p.nodeFirstTile[node];
+        if (left < 0) {
+          tile = first;
           keepLeaf = tile != rowTile;
           if (pure >= 0)
             tile |= kPureColumnTile;
@@ -305,8 +327,8 @@ __device__ void collectCandidates(const PassParams &p, const Metric &m, const We
     }
     if (expand) {
       const int at = frontLen + 2 * __popc(inner & below);
-      sh.frontNode[at] = p.nodeLeft[node];
-      sh.frontNode[at + 1] = p.nodeRight[node];
+      sh.frontNode[at] = left;
+      sh.frontNode[at + 1] = right;
     }
     listLen += __popc(leaves);
     frontLen += 2 * __popc(inner);

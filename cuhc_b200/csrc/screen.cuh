@@ -593,9 +593,10 @@ __global__ void __launch_bounds__(kThreads, 2)
           const float *cVal = reinterpret_cast<const float *>(cOrig + 2 * kTile);
           const bool mask = maskPass && !oneHot && !(rowPure >= 0 && colPure);
           const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * kTile);
-          // Row minimum of D' (own component excluded when masking): two
-          // 32-column loads in flight per wait, eight independent chains.
-          float mn;
+          // Minimum of D' over each 32-column chunk of the row (own component
+          // excluded when masking): two chunk loads in flight per wait, two
+          // independent chains per chunk.
+          float chunkMin[4];
           {
             float part[8];
 #pragma unroll
@@ -613,27 +614,30 @@ __global__ void __launch_bounds__(kThreads, 2)
                 for (int q = 0; q < 16; ++q) {
                   const uint32_t *src = q < 8 ? a : b;
                   const int c = (q & 7) * 4;
+                  const int chain = 4 * half + (q < 8 ? 0 : 2) + (q & 1);
                   const int4 cc = reinterpret_cast<const int4 *>(cComp)[half * 16 + q];
-                  part[q & 7] = min3(part[q & 7],
+                  part[chain] = min3(part[chain],
                                      cc.x != myComp ? __uint_as_float(src[c]) : INFINITY,
                                      cc.y != myComp ? __uint_as_float(src[c + 1]) : INFINITY);
-                  part[q & 7] = min3(part[q & 7],
+                  part[chain] = min3(part[chain],
                                      cc.z != myComp ? __uint_as_float(src[c + 2]) : INFINITY,
                                      cc.w != myComp ? __uint_as_float(src[c + 3]) : INFINITY);
                 }
               } else {
 #pragma unroll
                 for (int c = 0; c < 32; c += 2) {
-                  part[(c >> 1) & 7] = min3(part[(c >> 1) & 7], __uint_as_float(a[c]),
-                                            __uint_as_float(a[c + 1]));
-                  part[(c >> 1) & 7] = min3(part[(c >> 1) & 7], __uint_as_float(b[c]),
-                                            __uint_as_float(b[c + 1]));
+                  const int chain = 4 * half + ((c >> 1) & 1);
+                  part[chain] = min3(part[chain], __uint_as_float(a[c]), __uint_as_float(a[c + 1]));
+                  part[chain + 2] =
+                      min3(part[chain + 2], __uint_as_float(b[c]), __uint_as_float(b[c + 1]));
                 }
               }
             }
-            mn = fminf(fminf(min3(part[0], part[1], part[2]), min3(part[3], part[4], part[5])),
-                       fminf(part[6], part[7]));
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+              chunkMin[q] = fminf(part[2 * q], part[2 * q + 1]);
           }
+          const float mn = fminf(fminf(chunkMin[0], chunkMin[1]), fminf(chunkMin[2], chunkMin[3]));
           float Fs = F + kScreenAbsSlack;
           const bool want = myValid && mn <= Fs;
           if (__any_sync(0xffffffffu, want)) {
@@ -641,8 +645,13 @@ __global__ void __launch_bounds__(kThreads, 2)
             float v[32];
 #pragma unroll 1
             for (int chunk = 0; chunk < 4; ++chunk) {
+              // Only chunks holding a value within some row's bound are read
+              // again (the load is warp-wide, so the choice is too).
+              const bool wantChunk = want && chunkMin[chunk] <= Fs;
+              if (!__any_sync(0xffffffffu, wantChunk))
+                continue;
               tmemLoad32(taddr + chunk * 32, v);
-              if (!want)
+              if (!wantChunk)
                 continue;
               unsigned candidates = 0;
 #pragma unroll
