@@ -266,72 +266,88 @@ template <class Metric, class Weight>
 __device__ void collectCandidates(const PassParams &p, const Metric &m, const Weight &w,
                                   PassState &sh, const float *rowLow, const float *rowHigh,
                                   int rowTile, int rowPure, float rowMinValue, float slack) {
+  constexpr int kWidth = 2; // nodes per lane per step of the walk
   const int lane = threadIdx.x & 31;
   const float thr = sh.thrTile;
   int listLen = 0;
   int frontLen = sh.frontLen;
-  while (frontLen > 0 && listLen <= kListCap - 32) {
-    const int take = min(32, min(frontLen, kFrontierCap - frontLen));
+  while (frontLen > 0 && listLen <= kListCap - 32 * kWidth) {
+    const int take = min(32 * kWidth, min(frontLen, kFrontierCap - frontLen));
     if (take == 0) {
       if (lane == 0)
         sh.overflow = 1;
       break;
     }
-    int node = -1;
-    if (lane < take)
-      node = sh.frontNode[frontLen - 1 - lane];
+    int node[kWidth];
+#pragma unroll
+    for (int h = 0; h < kWidth; ++h)
+      node[h] = lane + 32 * h < take ? sh.frontNode[frontLen - 1 - lane - 32 * h] : -1;
     __syncwarp();
     frontLen -= take;
-    bool keepLeaf = false, expand = false;
-    int tile = -1;
-    float lb = 0.0f;
-    int left = -1, right = -1;
-    if (node >= 0) {
-      // Every field of the node is loaded before any is used: one round
-      // trip to L2 per step of the walk.
-      const int pure = p.nodePure ? __ldg(p.nodePure + node) : -1;
-      left = __ldg(p.nodeLeft + node);
-      right = __ldg(p.nodeRight + node);
-      const int first = __ldg(p.nodeFirstTile + node);
-      const float v = p.nodeMinValue ? __ldg(p.nodeMinValue + node) : 0.0f;
-      const bool skip = rowPure >= 0 && pure == rowPure;
-      if (!skip && p.prune && Metric::kBoxBound) {
-        typename Metric::Acc acc = m.init();
-        const float *lo = p.nodeLow + (size_t)node * p.d, *hi = p.nodeHigh + (size_t)node * p.d;
-#pragma unroll 8
-        for (int f = 0; f < p.d; ++f) {
-          const float gap =
-              fmaxf(0.0f, fmaxf(__ldg(lo + f) - rowHigh[f], rowLow[f] - __ldg(hi + f)));
-          acc = m.accumulate(acc, gap, 0.0f);
-        }
-        lb = w.lowerBound(m.finalize(acc), rowMinValue, v) * slack;
-      }
-      if (!skip && lb <= thr) {
-        if (left < 0) {
-          tile = first;
-          keepLeaf = tile != rowTile;
-          if (pure >= 0)
-            tile |= kPureColumnTile;
-        } else {
-          expand = true;
+    // Every field of every node of the step is loaded before any is used:
+    // one round trip to L2 per step of the walk.
+    int pure[kWidth], left[kWidth], right[kWidth], first[kWidth];
+    float value[kWidth];
+    typename Metric::Acc acc[kWidth];
+#pragma unroll
+    for (int h = 0; h < kWidth; ++h) {
+      const int q = max(node[h], 0);
+      pure[h] = p.nodePure ? __ldg(p.nodePure + q) : -1;
+      left[h] = __ldg(p.nodeLeft + q);
+      right[h] = __ldg(p.nodeRight + q);
+      first[h] = __ldg(p.nodeFirstTile + q);
+      value[h] = p.nodeMinValue ? __ldg(p.nodeMinValue + q) : 0.0f;
+      acc[h] = m.init();
+    }
+    const bool box = p.prune && Metric::kBoxBound;
+    if (box) {
+#pragma unroll 4
+      for (int f = 0; f < p.d; ++f) {
+        const float rl = rowLow[f], rh = rowHigh[f];
+#pragma unroll
+        for (int h = 0; h < kWidth; ++h) {
+          const size_t at = (size_t)max(node[h], 0) * p.d + f;
+          const float gap = fmaxf(0.0f, fmaxf(__ldg(p.nodeLow + at) - rh, rl - __ldg(p.nodeHigh + at)));
+          acc[h] = m.accumulate(acc[h], gap, 0.0f);
         }
       }
     }
-    const unsigned leaves = __ballot_sync(0xffffffffu, keepLeaf);
-    const unsigned inner = __ballot_sync(0xffffffffu, expand);
-    const unsigned below = (1u << lane) - 1;
-    if (keepLeaf) {
-      const int at = listLen + __popc(leaves & below);
-      sh.listTile[at] = tile;
-      sh.listLb[at] = lb;
+#pragma unroll
+    for (int h = 0; h < kWidth; ++h) {
+      bool keepLeaf = false, expand = false;
+      int tile = -1;
+      float lb = 0.0f;
+      if (node[h] >= 0) {
+        const bool skip = rowPure >= 0 && pure[h] == rowPure;
+        if (!skip && box)
+          lb = w.lowerBound(m.finalize(acc[h]), rowMinValue, value[h]) * slack;
+        if (!skip && lb <= thr) {
+          if (left[h] < 0) {
+            tile = first[h];
+            keepLeaf = tile != rowTile;
+            if (pure[h] >= 0)
+              tile |= kPureColumnTile;
+          } else {
+            expand = true;
+          }
+        }
+      }
+      const unsigned leaves = __ballot_sync(0xffffffffu, keepLeaf);
+      const unsigned inner = __ballot_sync(0xffffffffu, expand);
+      const unsigned below = (1u << lane) - 1;
+      if (keepLeaf) {
+        const int at = listLen + __popc(leaves & below);
+        sh.listTile[at] = tile;
+        sh.listLb[at] = lb;
+      }
+      if (expand) {
+        const int at = frontLen + 2 * __popc(inner & below);
+        sh.frontNode[at] = left[h];
+        sh.frontNode[at + 1] = right[h];
+      }
+      listLen += __popc(leaves);
+      frontLen += 2 * __popc(inner);
     }
-    if (expand) {
-      const int at = frontLen + 2 * __popc(inner & below);
-      sh.frontNode[at] = left;
-      sh.frontNode[at + 1] = right;
-    }
-    listLen += __popc(leaves);
-    frontLen += 2 * __popc(inner);
     __syncwarp();
   }
   if (lane == 0) {
