@@ -1,8 +1,9 @@
 """Builds cuhc_b200/libcuhc.so from csrc/ for sm_100a (in-tree, no JIT).
 
 Each translation unit compiles in parallel; the shared library is linked
-with nvcc. Rebuilds only what changed (a unit is stale when it or any header
-in csrc/ is newer than its object).
+with nvcc. Rebuilds only what changed: a unit is stale when it, or a header
+it includes (directly or through other csrc/ headers), is newer than its
+object.
 
     python -m cuhc_b200.build [--force] [--verbose]
 """
@@ -10,6 +11,7 @@ in csrc/ is newer than its object).
 import concurrent.futures
 import os
 import pathlib
+import re
 import subprocess
 import sys
 
@@ -28,9 +30,23 @@ def _sources():
     return sorted(SRC.glob("*.cu")) + sorted(SRC.glob("*.cpp"))
 
 
-def _headers_mtime():
-    headers = list(SRC.glob("*.cuh")) + list(SRC.glob("*.h"))
-    return max((h.stat().st_mtime for h in headers), default=0.0)
+_INCLUDE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.MULTILINE)
+
+
+def _newest_dependency(source, cache):
+    """Latest modification time of `source` and every csrc/ header it reaches
+    through quoted includes."""
+    seen, stack, newest = set(), [source], 0.0
+    while stack:
+        path = stack.pop()
+        if path in seen or not path.exists():
+            continue
+        seen.add(path)
+        newest = max(newest, path.stat().st_mtime)
+        if path not in cache:
+            cache[path] = [SRC / name for name in _INCLUDE.findall(path.read_text())]
+        stack.extend(cache[path])
+    return newest
 
 
 def _compile(source, verbose):
@@ -50,14 +66,18 @@ def _compile(source, verbose):
 def build(force=False, verbose=False, jobs=None):
     """Compiles stale units and links libcuhc.so; returns its path."""
     OBJ.mkdir(exist_ok=True)
-    headers = _headers_mtime()
     sources = _sources()
+    cache = {}
     stale = []
     for source in sources:
         obj = OBJ / (source.name + ".o")
-        if (force or not obj.exists() or obj.stat().st_mtime < source.stat().st_mtime
-                or obj.stat().st_mtime < headers):
+        if (force or not obj.exists()
+                or obj.stat().st_mtime < _newest_dependency(source, cache)):
             stale.append(source)
+    # Objects of units that no longer exist must not be linked.
+    for obj in OBJ.glob("*.o"):
+        if not (SRC / obj.name[:-2]).exists():
+            obj.unlink()
     logs = []
     if stale:
         with concurrent.futures.ThreadPoolExecutor(jobs or os.cpu_count() or 4) as pool:

@@ -23,19 +23,26 @@ int pairwiseDistances(const float *A, int nA, const float *B, int nB, int d, con
 
 } // namespace cuhc
 
-#define CUHC_INSTANTIATE_METRIC(M)                                                                 \
+// Three parts per metric, one translation unit each (inst_<metric>_<part>.cu),
+// so that the slowest metric (minkowski: exp2f / log2f per pair in every
+// kernel) does not serialise the build.
+#define CUHC_INSTANTIATE_MST(M)                                                                    \
   template int cuhc::boruvkaMst<M, cuhc::PlainWeight>(                                             \
       cuhc::SpatialIndex &, const M &, const cuhc::PlainWeight &, bool, cuhc::DeviceEdges &,       \
-      cuhc::PassStats *, cudaStream_t, cuhc::RadiusLog *);                                         \
+      cuhc::PassStats *, cudaStream_t, cuhc::RadiusLog *);
+
+#define CUHC_INSTANTIATE_MREACH(M)                                                                 \
   template int cuhc::boruvkaMst<M, cuhc::MutualReachWeight>(                                       \
       cuhc::SpatialIndex &, const M &, const cuhc::MutualReachWeight &, bool, cuhc::DeviceEdges &, \
-      cuhc::PassStats *, cudaStream_t, cuhc::RadiusLog *);                                                            \
+      cuhc::PassStats *, cudaStream_t, cuhc::RadiusLog *);
+
+#define CUHC_INSTANTIATE_CORE(M)                                                                   \
   template int cuhc::coreDistances<M>(cuhc::SpatialIndex &, const M &, int, bool, float *,         \
-                                      cuhc::PassStats *, cudaStream_t, const int *);                            \
+                                      cuhc::PassStats *, cudaStream_t, const int *);               \
   template bool cuhc::screenable<M>(cuhc::SpatialIndex &, int);                                    \
   template float cuhc::timeKnnSample<M>(cuhc::SpatialIndex &, const M &, int, bool, int, float *,  \
-                                        cudaStream_t);                                           \
-  template int cuhc::coreDistancesRadix<M>(cuhc::SpatialIndex &, const M &, int, float *,        \
-                                           cudaStream_t);                                        \
+                                        cudaStream_t);                                             \
+  template int cuhc::coreDistancesRadix<M>(cuhc::SpatialIndex &, const M &, int, float *,          \
+                                           cudaStream_t);                                          \
   template int cuhc::pairwiseDistances<M>(const float *, int, const float *, int, int, const M &,  \
                                           float *, cudaStream_t);

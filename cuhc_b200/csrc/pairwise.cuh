@@ -16,7 +16,7 @@ template <class Metric, int KC>
 __global__ void __launch_bounds__(kThreads, 2)
     pairwiseKernel(const float *__restrict__ tiledA, const float *__restrict__ tiledB, int nA,
                    int nB, int numChunks, Metric m, float *__restrict__ out) {
-  extern __shared__ __align__(16) float dyn[];
+  extern __shared__ __align__(128) float dyn[];
   float *sA = dyn, *sB = dyn + KC * kTile;
   const TileGeom g;
   const int I = blockIdx.y, J = blockIdx.x;
