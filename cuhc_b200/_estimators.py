@@ -1,6 +1,11 @@
-"""scikit-learn compatible AgglomerativeClustering on the exact GPU merge
-trees (same parameters, defaults and fitted attributes as
-sklearn.cluster.AgglomerativeClustering, plus `algorithm`)."""
+"""AgglomerativeClustering on the exact GPU merge trees.
+
+Follows the documented contract of sklearn.cluster.AgglomerativeClustering:
+the same constructor parameters and defaults (plus `algorithm`, the tree
+builder of `linkage`), the same fitted attributes, and the same flat cut --
+with `distance_threshold` set, every merge whose height is at or above the
+threshold is undone, so the cut keeps the merges strictly below it.
+"""
 
 import numbers
 
@@ -14,7 +19,7 @@ from ._linkage import LINKAGE_IDS, cut_tree, linkage, resolve_algorithm, validat
 class AgglomerativeClustering(ClusterMixin, BaseEstimator):
     """Exact agglomerative clustering on the GPU.
 
-    Parameters: n_clusters (or distance_threshold, exactly one of them),
+    Parameters: n_clusters (or distance_threshold: set exactly one),
     metric, linkage ("ward", "complete", "average", "single"),
     compute_distances, algorithm ("auto", "dense", "mst", "rnn", "nn_chain").
     Fitted: labels_, n_clusters_, children_, distances_ (with
@@ -31,37 +36,48 @@ class AgglomerativeClustering(ClusterMixin, BaseEstimator):
         self.compute_distances = compute_distances
         self.algorithm = algorithm
 
-    def _check_params(self):
-        if (self.n_clusters is None) == (self.distance_threshold is None):
+    def _flat_cut_size(self, heights, n_samples):
+        """Clusters of the flat cut: n_clusters, or the points minus the
+        merges strictly below distance_threshold."""
+        if self.distance_threshold is None:
+            return int(self.n_clusters)
+        below = np.asarray(heights) < self.distance_threshold
+        return n_samples - int(below.sum())
+
+    def _validate(self, n_samples):
+        by_count = self.n_clusters is not None
+        by_height = self.distance_threshold is not None
+        if by_count == by_height:
+            # scikit-learn's own wording: callers match on it.
             raise ValueError("Exactly one of n_clusters and distance_threshold has to be set, "
                              "and the other needs to be None.")
-        if self.n_clusters is not None and (
-                not isinstance(self.n_clusters, numbers.Integral) or self.n_clusters < 1):
-            raise ValueError(f"n_clusters must be a positive integer, got {self.n_clusters!r}")
         if self.linkage not in LINKAGE_IDS:
-            raise ValueError(f"linkage must be one of {list(LINKAGE_IDS)}, got {self.linkage!r}")
+            raise ValueError(f"unknown linkage {self.linkage!r}; expected one of "
+                             f"{sorted(LINKAGE_IDS)}")
         validate_linkage(self.linkage, self.metric)
         resolve_algorithm(self.algorithm, self.linkage)
+        if by_count:
+            valid = isinstance(self.n_clusters, numbers.Integral) and self.n_clusters >= 1
+            if not valid:
+                raise ValueError(f"n_clusters must be an integer >= 1, got {self.n_clusters!r}")
+            if self.n_clusters > n_samples:
+                raise ValueError(f"n_clusters={self.n_clusters} exceeds the {n_samples} samples")
 
     def fit(self, X, y=None):
-        self._check_params()
-        X = as_points(X, "X")
-        n = X.shape[0]
-        if self.n_clusters is not None and self.n_clusters > n:
-            raise ValueError(f"Cannot extract more clusters ({self.n_clusters}) than samples ({n})")
-        Z = linkage(X, method=self.linkage, metric=self.metric, algorithm=self.algorithm)
-        if self.distance_threshold is not None:
-            # Merges at or above the threshold split clusters (sklearn's rule).
-            self.n_clusters_ = int(np.count_nonzero(Z[:, 2] >= self.distance_threshold)) + 1
-        else:
-            self.n_clusters_ = int(self.n_clusters)
-        self.labels_ = cut_tree(Z, n - self.n_clusters_)
-        self.children_ = Z[:, :2].astype(np.intp)
-        if self.compute_distances or self.distance_threshold is not None:
-            self.distances_ = Z[:, 2].copy()
-        self.n_leaves_ = n
-        self.n_features_in_ = X.shape[1]
-        self.n_connected_components_ = 1
+        points = as_points(X, "X")
+        n_samples = points.shape[0]
+        self._validate(n_samples)
+        tree = linkage(points, method=self.linkage, metric=self.metric, algorithm=self.algorithm)
+        heights = tree[:, 2]
+        clusters = self._flat_cut_size(heights, n_samples)
+        self.n_leaves_ = n_samples
+        self.n_features_in_ = points.shape[1]
+        self.n_connected_components_ = 1  # every tree here joins all points
+        self.children_ = tree[:, :2].astype(np.intp)
+        self.n_clusters_ = clusters
+        self.labels_ = cut_tree(tree, n_samples - clusters)
+        if self.distance_threshold is not None or self.compute_distances:
+            self.distances_ = np.array(heights, dtype=np.float64)
         return self
 
     def fit_predict(self, X, y=None):

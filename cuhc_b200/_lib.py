@@ -13,7 +13,7 @@ _LIB_PATH = pathlib.Path(__file__).resolve().parent / "libcuhc.so"
 
 if not _LIB_PATH.exists():
     raise ImportError(
-        f"{_LIB_PATH} is missing; build it with `python -m cuhc_b200.build` "
+        f"{_LIB_PATH} is missing; build it with `python cuhc_b200/build.py` "
         "(nvcc for sm_100a). cuhc_b200 has no CPU fallback.")
 
 lib = ctypes.CDLL(str(_LIB_PATH))
@@ -64,6 +64,12 @@ lib.cuhc_set_timing.restype = _int
 lib.cuhc_set_timing.argtypes = [_int]
 lib.cuhc_kernel_timing.restype = _int
 lib.cuhc_kernel_timing.argtypes = [_f64, _u64, _u64, _int]
+lib.cuhc_set_screen_audit.restype = _int
+lib.cuhc_set_screen_audit.argtypes = [_int]
+lib.cuhc_screen_audit.restype = _int
+lib.cuhc_screen_audit.argtypes = [_f64, _int]
+lib.cuhc_wait_selftest.restype = _int
+lib.cuhc_wait_selftest.argtypes = [_int, _int, _int]
 
 PRUNE_MODES = {"auto": 0, "always": 1, "never": 2}
 SCREEN_MODES = {"auto": 0, "on": 1, "off": 2}
@@ -147,3 +153,29 @@ def kernel_timing():
     launches, tiles = (ctypes.c_uint64 * 4)(), (ctypes.c_uint64 * 4)()
     check(lib.cuhc_kernel_timing(ms, launches, tiles, 4))
     return {TIMER_KINDS[i]: (ms[i], int(launches[i]), int(tiles[i])) for i in range(4)}
+
+
+AUDIT_FIELDS = ("pairs", "violations", "min_slack", "max_bound_gap_rel_norms", "max_bound_gap_abs",
+                "max_exact_abs", "max_exact_rel")
+
+
+def set_screen_audit(on):
+    """Audit of the tensor-core screen (off by default): every pair of every
+    screened tile is also checked against the reference FP32 distance and an
+    FP64 recomputation. Results never change; audited passes are slower."""
+    check(lib.cuhc_set_screen_audit(1 if on else 0))
+
+
+def screen_audit():
+    """Audit results since the last call (resets): pairs audited,
+    violations of the screen's guarantee D' <= s (must be 0), the smallest
+    slack (s - D') / (e (|x|^2 + |y|^2)) (>= 0 required; about 0.5 or more
+    means the modelled error bound holds with room), the largest gap of the
+    screened bound below the FP64 value (relative to the norms, and
+    absolute), and the largest absolute / relative error of the reference
+    FP32 squared distance against FP64. NaN where nothing was observed."""
+    out = (ctypes.c_double * len(AUDIT_FIELDS))()
+    check(lib.cuhc_screen_audit(out, len(AUDIT_FIELDS)))
+    values = [float(x) for x in out]
+    values[0], values[1] = int(values[0]), int(values[1])
+    return dict(zip(AUDIT_FIELDS, values))

@@ -26,7 +26,7 @@ def validate_linkage(method, metric):
         raise ValueError(f"ward linkage requires metric='euclidean', got {metric!r}")
 
 
-def resolve_algorithm(algorithm, method, num_points=None):
+def resolve_algorithm(algorithm, method):
     """The algorithm that builds `method`; "auto" is the fastest exact one."""
     if algorithm == "auto":
         return _AUTO.get(method, "dense")
@@ -55,7 +55,7 @@ def linkage(X, method="single", metric="euclidean", p=2.0, *, algorithm="auto"):
     n = X.shape[0]
     # Ward heights grow with cluster size: 2 n_a n_b / (n_a + n_b) <= n.
     check_distance_range(X, metric, p, scale=n if method == "ward" else 1.0)
-    algorithm = resolve_algorithm(algorithm, method, n)
+    algorithm = resolve_algorithm(algorithm, method)
     tree = np.empty((max(n - 1, 0), 4), dtype=np.float64)
     if n == 1:
         return tree

@@ -5,7 +5,7 @@ with nvcc. Rebuilds only what changed: a unit is stale when it, or a header
 it includes (directly or through other csrc/ headers), is newer than its
 object.
 
-    python -m cuhc_b200.build [--force] [--verbose]
+    python cuhc_b200/build.py [--force] [--verbose]
 """
 
 import concurrent.futures

@@ -109,14 +109,16 @@ __device__ __forceinline__ bool mbarrierTryWaitSuspend(uint64_t *bar, uint32_t p
 // Waits for the barrier's phase `phase` to complete, suspended in between
 // (a waiting warp takes no issue slots from the warps doing the work); false
 // if a second of wall-clock time (or the iteration limit) ran out first.
-__device__ __forceinline__ bool mbarrierWait(uint64_t *bar, uint32_t phase) {
+// limitNs shortens the limit (the bounded-wait self-test only).
+__device__ __forceinline__ bool mbarrierWait(uint64_t *bar, uint32_t phase,
+                                             uint64_t limitNs = kWaitLimitNs) {
   if (mbarrierTryWait(bar, phase))
     return true;
   const uint64_t start = globalTimerNs();
   for (long long spins = 0; spins < kSpinLimit; ++spins) {
     if (mbarrierTryWaitSuspend(bar, phase, 100000u))
       return true;
-    if (globalTimerNs() - start > kWaitLimitNs)
+    if (globalTimerNs() - start > limitNs)
       return false;
   }
   return false;

@@ -206,6 +206,7 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
   p.tilesComputed = tiles.get();
   p.error = error.get();
   p.screenStats = screenCounters();
+  p.screenAudit = screenAuditWords();
   p.rootOfTile = index.numInstances > 1 ? index.rootOfTile.get() : nullptr;
 
   const bool screened = useScreen<Metric>(index.d, 0) && index.extentsWithin(kScreenMaxExtent);
@@ -472,6 +473,7 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
   p.tilesComputed = tiles.get();
   p.error = error.get();
   p.screenStats = screenCounters();
+  p.screenAudit = screenAuditWords();
   p.rootOfTile = index.numInstances > 1 ? index.rootOfTile.get() : nullptr;
   {
     const bool screened =

@@ -13,6 +13,7 @@
 // iteration limit. A wait that runs out records kErrorTimeout and the block
 // returns; the host reports the error. The launch is cooperative, so all
 // blocks are co-resident.
+#include "asyncload.cuh"
 #include "profiling.cuh"
 #include "rnn.cuh"
 
@@ -42,8 +43,9 @@ __device__ __forceinline__ bool lessLoc(float da, int ia, float db, int ib) {
 }
 
 // Grid barrier with a bounded wait. Returns false (everyone in the block)
-// when the wait ran out.
-__device__ bool gridBarrier(const ChainState &s) {
+// when the wait ran out (after spinLimit polls; only the bounded-wait
+// self-test passes a shorter limit).
+__device__ bool gridBarrier(const ChainState &s, long long spinLimit = kSpinLimit) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -58,7 +60,7 @@ __device__ bool gridBarrier(const ChainState &s) {
     } else {
       long long spins = 0;
       while (*gen == g) {
-        if (++spins > kSpinLimit) {
+        if (++spins > spinLimit) {
           atomicCAS(s.error, 0, (int)kErrorTimeout);
           ok = 0;
           break;
@@ -82,6 +84,32 @@ __device__ __forceinline__ float wardSquared(const float *a, const float *b, int
     squared = fmaf(diff, diff, squared);
   }
   return 2.0f * sa * sb / (sa + sb) * squared;
+}
+
+// Bounded-wait self-test (cuhc_wait_selftest). The grid barrier above with
+// block `missing` returning before it arrives: every other block's wait runs
+// out after spinLimit polls and records kErrorTimeout. missing < 0: all
+// arrive and the barrier completes.
+__global__ void barrierSelftestKernel(ChainState s, int missing, long long spinLimit) {
+  if ((int)blockIdx.x == missing)
+    return;
+  gridBarrier(s, spinLimit);
+}
+
+// The pass kernels' mbarrier wait on a barrier whose expected arrival never
+// comes (missing != 0: nothing arrives) or has come (missing == 0): a wait
+// that runs out records kErrorTimeout.
+__global__ void mbarrierSelftestKernel(int missing, unsigned long long limitNs, int *error) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbarrierInit(&bar, 1);
+    fenceBarrierInit();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !missing)
+    mbarrierArrive(&bar, 1);
+  if (!mbarrierWait(&bar, 0, limitNs))
+    atomicCAS(error, 0, (int)kErrorTimeout);
 }
 
 __global__ void __launch_bounds__(kChainThreads) chainKernel(ChainState s) {
@@ -299,3 +327,47 @@ int chainOnClusters(const float *centroids, const int *sizes, int m, int d, cuda
 }
 
 } // namespace cuhc
+
+// Self-test of the bounded device waits: a wait whose arrival never comes
+// must run out and report kErrorTimeout, leaving the context usable; with
+// every arrival made it must complete. No fault, trap or unbounded spin is
+// involved: the missing arrival is a block that returns early (grid barrier)
+// or an arrival that is never made (mbarrier).
+extern "C" int cuhc_wait_selftest(int kind, int missing, int limitMicroseconds) {
+  using namespace cuhc;
+  if (kind < 0 || kind > 1 || limitMicroseconds < 1 || limitMicroseconds > 1000000)
+    return kErrorInvalidShape;
+  cudaStream_t stream = nullptr;
+  StatusChain st;
+  st((int)cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  DeviceBuffer<unsigned int> words;
+  CUHC_TRY(st, words.allocate(3, stream)); // barrier count, generation, error
+  CUHC_TRY(st, cudaMemsetAsync(words.get(), 0, words.bytes(), stream));
+  int *error = reinterpret_cast<int *>(words.get() + 2);
+  if (st.ok() && kind == 0) {
+    ChainState s{};
+    s.barrierCount = words.get();
+    s.barrierGen = words.get() + 1;
+    s.error = error;
+    int absent = missing ? 1 : -1;
+    // A poll takes at least the 64 ns nap: about 8 polls per microsecond.
+    long long polls = 8ll * limitMicroseconds;
+    void *args[] = {&s, &absent, &polls};
+    CUHC_TRY(st, cudaLaunchCooperativeKernel((void *)barrierSelftestKernel, 4, 32, args, 0,
+                                             stream));
+    noteLaunch();
+  } else if (st.ok()) {
+    mbarrierSelftestKernel<<<1, 32, 0, stream>>>(missing, 1000ull * limitMicroseconds, error);
+    noteLaunch();
+    CUHC_TRY(st, cudaGetLastError());
+  }
+  int recorded = 0;
+  CUHC_TRY(st, cudaMemcpyAsync(&recorded, error, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  CUHC_TRY(st, cudaStreamSynchronize(stream));
+  words.release();
+  if (stream) {
+    cudaStreamSynchronize(stream);
+    cudaStreamDestroy(stream);
+  }
+  return st.ok() ? recorded : st.code;
+}

@@ -157,6 +157,7 @@ struct PassParams {
   unsigned long long *tilesComputed;
   int *error;
   unsigned long long *screenStats; // ScreenCounter sums (null: not counted)
+  unsigned long long *screenAudit; // ScreenAuditWord words (null: no audit)
   const int *rootOfTile;  // traversal root per row tile (null: node 0)
   const int *coreRank;    // knn-mode rank per position, 0 = core 0 (null: k for all)
   // Nearest mode: per-position cap on the row threshold (a proposed radius);

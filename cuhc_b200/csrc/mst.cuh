@@ -43,7 +43,8 @@ bool mergesFormTree(const std::vector<int> &u, const std::vector<int> &v,
                     const std::vector<float> &w, int n);
 
 // Borůvka over the points of an index (Metric x Weight instantiations in
-// boruvka_*.cu). Fills edges with the n-1 MST edges (original indices).
+// inst_<metric>_mst.cu and inst_<metric>_mreach.cu). Fills edges with the
+// n-1 MST edges (original indices).
 template <class Metric, class Weight>
 int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, bool prune,
                DeviceEdges &edges, PassStats *stats, cudaStream_t stream,

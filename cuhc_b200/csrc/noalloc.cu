@@ -44,7 +44,7 @@ int scratchAddress(void **out) {
   if (e != cudaSuccess)
     return (int)e;
   if (device < 0 || device >= kMaxDevices)
-    return kErrorTooLarge;
+    return (int)cudaErrorInvalidDevice; // beyond the per-device address cache
   std::lock_guard<std::mutex> lock(gScratchMutex);
   if (!gScratchAddress[device]) {
     void *ptr = nullptr;

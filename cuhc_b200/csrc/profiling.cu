@@ -1,5 +1,9 @@
 #include "profiling.cuh"
 
+#include <cmath>
+
+#include "common.cuh"
+
 #include <atomic>
 #include <mutex>
 
@@ -13,6 +17,20 @@ unsigned long long gCount[kNumTimers] = {}, gTiles[kNumTimers] = {};
 } // namespace
 
 __device__ unsigned long long gScreenCounterArray[kNumScreenCounters];
+__device__ unsigned long long gScreenAuditArray[kNumAuditWords];
+
+namespace {
+std::atomic<int> gAudit{0};
+} // namespace
+
+unsigned long long *screenAuditWords() {
+  if (gAudit.load() == 0)
+    return nullptr;
+  void *ptr = nullptr;
+  if (cudaGetSymbolAddress(&ptr, gScreenAuditArray) != cudaSuccess)
+    return nullptr;
+  return static_cast<unsigned long long *>(ptr);
+}
 
 void noteLaunch(int count) { gLaunches.fetch_add((unsigned long long)count); }
 bool timingEnabled() { return gTiming.load() != 0; }
@@ -94,6 +112,41 @@ int cuhc_screen_counters(unsigned long long *out, int count) {
   }
   for (int i = 0; i < count && i < cuhc::kNumScreenCounters; ++i)
     out[i] = host[i];
+  return (int)e;
+}
+
+// Screen audit on (1) or off (0); test and measurement hook, off by default
+// (an audited pass evaluates every pair of its tiles twice more, in FP32 and
+// FP64). Results of the passes never change.
+int cuhc_set_screen_audit(int on) {
+  if (on < 0 || on > 1)
+    return cuhc::kErrorInvalidAlgorithm;
+  cuhc::gAudit.store(on);
+  return 0;
+}
+
+// The audit words of the current device since the last call, decoded (first
+// `count` of): pairs, violations, min slack, max bound gap (relative to the
+// norms), max bound gap (absolute), max exact abs error, max exact rel error;
+// NaN where nothing was observed. Resets them.
+int cuhc_screen_audit(double *out, int count) {
+  unsigned long long host[cuhc::kNumAuditWords] = {};
+  cudaError_t e = cudaMemcpyFromSymbol(host, cuhc::gScreenAuditArray, sizeof(host));
+  if (e == cudaSuccess) {
+    const unsigned long long zero[cuhc::kNumAuditWords] = {};
+    e = cudaMemcpyToSymbol(cuhc::gScreenAuditArray, zero, sizeof(zero));
+  }
+  for (int i = 0; i < count && i < cuhc::kNumAuditWords; ++i) {
+    const unsigned long long v = host[i];
+    if (i == cuhc::kAuditPairs || i == cuhc::kAuditViolations)
+      out[i] = (double)v;
+    else if (v == 0)
+      out[i] = NAN;
+    else if (i == cuhc::kAuditMinSlack)
+      out[i] = cuhc::orderedFloat(~(uint32_t)v);
+    else
+      out[i] = cuhc::orderedFloat((uint32_t)v);
+  }
   return (int)e;
 }
 

@@ -29,6 +29,27 @@ enum ScreenCounter : int { kScreenRechecks = 0, kScreenSlowRows = 1, kScreenIndi
 // Null when timing is off (the kernels then count nothing).
 unsigned long long *screenCounters();
 
+// Screen audit (cuhc_set_screen_audit): with it on, every screened tile also
+// checks each valid pair's tensor-core value D' against the reference FP32
+// squared distance s and an FP64 recomputation s64, and folds the results
+// into these device words: pairs audited, pairs with D' > s + 2^-70 (the
+// screen's guarantee broken; must stay 0), then minima / maxima stored as
+// order-preserving float bits (min: complemented) of
+//   slack      (s - D') / (e (|x|^2 + |y|^2)), x, y the centred coordinates
+//              and e the screen's margin; >= 0 is the guarantee, and the
+//              margin is twice the modelled error, so about 0.5 or more
+//              means the error model holds with room to spare;
+//   boundGap   (s64 - D') / (|x|^2 + |y|^2): how far below the exact value
+//              the screened bound sits, relative to the norms;
+//   boundAbs   s64 - D';
+//   exactAbs   |s - s64| and exactRel |s - s64| / s64 (s64 > 0): the
+//              reference FP32 chain's own error.
+enum ScreenAuditWord : int { kAuditPairs = 0, kAuditViolations = 1, kAuditMinSlack = 2,
+                             kAuditMaxBoundGap = 3, kAuditMaxBoundAbs = 4, kAuditMaxExactAbs = 5,
+                             kAuditMaxExactRel = 6, kNumAuditWords = 7 };
+// Null when the audit is off.
+unsigned long long *screenAuditWords();
+
 // RAII bracket around one pass launch; records only when timing is on.
 struct PassTimer {
   int kind;

@@ -282,6 +282,7 @@ int rnnWard(const float *devPoints, int n, int d, const RnnOptions &options, dou
     p.tilesComputed = tiles.get();
     p.error = error.get();
   p.screenStats = screenCounters();
+  p.screenAudit = screenAuditWords();
     WardWeight w;
     w.value = sizeF[cur].get();
     {

@@ -48,6 +48,7 @@
 
 #include <climits>
 #include <cmath>
+#include <type_traits>
 
 #include "passes.cuh"
 #include "umma.cuh"
@@ -190,7 +191,96 @@ __device__ __forceinline__ void buildColumnOperand(const float *raw, const int *
   storeOperandRow<kPad>(opB, j, val);
 }
 
-template <class Metric, class Weight, int KC, bool kKnn>
+// Audit of one computed tile (cuhc_set_screen_audit; one consumer warp, its
+// accumulator still held): every valid pair of the warp's rows -- a real
+// column point, and in Borůvka passes another component -- has its screened
+// value D' compared with the reference FP32 squared distance s (the chain the
+// exact path recomputes) and with an FP64 recomputation s64; the warp folds
+// the pair count, violations (D' > s + 2^-70) and the extrema described at
+// ScreenAuditWord into `words`. Off the timed path: nothing here runs unless
+// the audit is on, and it changes no result.
+template <class Metric, int KC, bool kKnn>
+__device__ __noinline__ void auditTile(unsigned long long *words, uint32_t taddr, const Metric &m,
+                                       const float *sA, const float *raw, const float *centre,
+                                       int myRow, bool rowValid, int myComp, int firstCol, int n,
+                                       const int *cOrig, const int *cComp, bool useComp,
+                                       float margin) {
+  unsigned long long pairs = 0, violations = 0;
+  float minSlack = INFINITY, maxGap = -INFINITY, maxAbs = -INFINITY, exactAbs = -INFINITY,
+        exactRel = -INFINITY;
+  float a[KC], x[KC];
+  double ni = 0.0;
+#pragma unroll
+  for (int k = 0; k < KC; ++k) {
+    a[k] = sA[k * kTile + myRow];
+    x[k] = a[k] - centre[k];
+    ni += (double)x[k] * (double)x[k];
+  }
+#pragma unroll 1
+  for (int chunk = 0; chunk < 4; ++chunk) {
+    float v[32];
+    tmemLoad32(taddr + chunk * 32, v);
+#pragma unroll 1
+    for (int c = 0; c < 32; ++c) {
+      const int jj = chunk * 32 + c;
+      if (!rowValid || firstCol + jj >= n || cOrig[jj] < 0)
+        continue;
+      if (!kKnn && (useComp ? cComp[jj] : cOrig[jj]) == myComp)
+        continue;
+      typename Metric::Acc acc = m.init();
+      double s64 = 0.0, nj = 0.0;
+#pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        const float b = raw[k * kTile + jj];
+        acc = m.accumulate(acc, a[k], b);
+        const double diff = (double)a[k] - (double)b;
+        s64 = fma(diff, diff, s64);
+        const float y = b - centre[k];
+        nj = fma((double)y, (double)y, nj);
+      }
+      const double s = (double)acc, dp = (double)v[c];
+      ++pairs;
+      if (dp > s + 0x1p-70)
+        ++violations;
+      const double norms = ni + nj;
+      if (norms > 0.0) {
+        minSlack = fminf(minSlack, (float)((s - dp) / ((double)margin * norms)));
+        maxGap = fmaxf(maxGap, (float)((s64 - dp) / norms));
+      }
+      maxAbs = fmaxf(maxAbs, (float)(s64 - dp));
+      exactAbs = fmaxf(exactAbs, (float)fabs(s - s64));
+      if (s64 > 0.0)
+        exactRel = fmaxf(exactRel, (float)(fabs(s - s64) / s64));
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off /= 2) {
+    pairs += __shfl_xor_sync(0xffffffffu, pairs, off);
+    violations += __shfl_xor_sync(0xffffffffu, violations, off);
+    minSlack = fminf(minSlack, __shfl_xor_sync(0xffffffffu, minSlack, off));
+    maxGap = fmaxf(maxGap, __shfl_xor_sync(0xffffffffu, maxGap, off));
+    maxAbs = fmaxf(maxAbs, __shfl_xor_sync(0xffffffffu, maxAbs, off));
+    exactAbs = fmaxf(exactAbs, __shfl_xor_sync(0xffffffffu, exactAbs, off));
+    exactRel = fmaxf(exactRel, __shfl_xor_sync(0xffffffffu, exactRel, off));
+  }
+  if ((threadIdx.x & 31) == 0 && pairs > 0) {
+    atomicAdd(words + kAuditPairs, pairs);
+    if (violations)
+      atomicAdd(words + kAuditViolations, violations);
+    if (minSlack < INFINITY)
+      atomicMax(words + kAuditMinSlack, (unsigned long long)(~orderedBits(minSlack)));
+    if (maxGap > -INFINITY)
+      atomicMax(words + kAuditMaxBoundGap, (unsigned long long)orderedBits(maxGap));
+    atomicMax(words + kAuditMaxBoundAbs, (unsigned long long)orderedBits(maxAbs));
+    atomicMax(words + kAuditMaxExactAbs, (unsigned long long)orderedBits(exactAbs));
+    if (exactRel > -INFINITY)
+      atomicMax(words + kAuditMaxExactRel, (unsigned long long)orderedBits(exactRel));
+  }
+}
+
+// kAudit: the audited variant (launched only while cuhc_set_screen_audit is
+// on), so that the audit costs the normal kernel nothing.
+template <class Metric, class Weight, int KC, bool kKnn, bool kAudit>
 __global__ void __launch_bounds__(kThreads, 2)
     screenKernel(PassParams p, Metric m, Weight w, float margin) {
   using L = ScreenLayout<KC>;
@@ -693,6 +783,9 @@ __global__ void __launch_bounds__(kThreads, 2)
               }
             }
           }
+          if (kAudit)
+            auditTile<Metric, KC, kKnn>(p.screenAudit, taddr, m, sA, raw, centre, myRow, myValid,
+                                        myComp, J * kTile, p.n, cOrig, cComp, useComp, margin);
           // The row's filter changes only through its own exact path or the
           // component's best (found by other blocks): refresh then, and every
           // eighth tile for the latter.
@@ -862,16 +955,20 @@ int launchScreen(const PassParams &p, const Metric &m, const Weight &w, int kc,
       noteLaunch();
       return (int)cudaGetLastError();
     };
-    switch (kc) {
-    case 4:
-      return run(screenKernel<Metric, Weight, 4, kKnn>);
-    case 8:
-      return run(screenKernel<Metric, Weight, 8, kKnn>);
-    case 16:
-      return run(screenKernel<Metric, Weight, 16, kKnn>);
-    default:
-      return run(screenKernel<Metric, Weight, 32, kKnn>);
-    }
+    auto byWidth = [&](auto audit) {
+      constexpr bool kAudit = decltype(audit)::value;
+      switch (kc) {
+      case 4:
+        return run(screenKernel<Metric, Weight, 4, kKnn, kAudit>);
+      case 8:
+        return run(screenKernel<Metric, Weight, 8, kKnn, kAudit>);
+      case 16:
+        return run(screenKernel<Metric, Weight, 16, kKnn, kAudit>);
+      default:
+        return run(screenKernel<Metric, Weight, 32, kKnn, kAudit>);
+      }
+    };
+    return p.screenAudit ? byWidth(std::true_type{}) : byWidth(std::false_type{});
   }
 }
 

@@ -2,9 +2,9 @@
 
     python -m cuhc_b200.train_radius [--n 1000000] [--seeds 10-19] [--out PATH]
 
-Data: the 16-feature recipe of `make_anisotropic_blobs` (50 Gaussian clusters
-sharing one random covariance with eigenvalues log-uniform in [0.05, 5], plus
-5% uniform noise) for each seed; every exact single-linkage Borůvka round of
+Data: the 16-feature recipe of `make_anisotropic_blobs` (50 Gaussian clusters,
+each with its own random covariance, eigenvalues log-uniform in [0.05, 5],
+plus 5% uniform noise) for each seed; every exact single-linkage Borůvka round of
 each data set contributes up to 20,000 random rows. Needs a GPU.
 """
 
@@ -14,19 +14,22 @@ import numpy as np
 
 
 def make_anisotropic_blobs(seed, n, d=16, centers=50, noise=0.05):
-    """centers clusters of equal weight, centres uniform in [-10, 10]^d,
-    covariance Q diag(l) Q^T (Q from the QR of a Gaussian matrix, l
-    log-uniform in [0.05, 5]), plus `noise` of the points uniform over the
-    clusters' bounding box; float32, shuffled."""
+    """centers clusters of equal weight, centres uniform in [-10, 10]^d, each
+    with its own random covariance Q diag(l) Q^T (Q from the QR of a Gaussian
+    matrix, l log-uniform in [0.05, 5]), plus `noise` of the points uniform
+    over the clusters' bounding box; float32, shuffled."""
     rng = np.random.default_rng(seed)
     n_noise = int(round(n * noise))
     m = n - n_noise
     centres = rng.uniform(-10.0, 10.0, (centers, d))
-    q, _ = np.linalg.qr(rng.standard_normal((d, d)))
-    lam = np.exp(rng.uniform(np.log(0.05), np.log(5.0), d))
-    transform = q * np.sqrt(lam)  # x = centre + transform @ z, covariance Q diag(lam) Q^T
+    transforms = np.empty((centers, d, d))
+    for c in range(centers):
+        q, _ = np.linalg.qr(rng.standard_normal((d, d)))
+        lam = np.exp(rng.uniform(np.log(0.05), np.log(5.0), d))
+        transforms[c] = q * np.sqrt(lam)  # x = centre + T z: covariance Q diag(lam) Q^T
     label = np.arange(m) % centers
-    pts = centres[label] + rng.standard_normal((m, d)) @ transform.T
+    z = rng.standard_normal((m, d))
+    pts = centres[label] + np.einsum("nij,nj->ni", transforms[label], z)
     lo, hi = pts.min(axis=0), pts.max(axis=0)
     X = np.vstack([pts, rng.uniform(lo, hi, (n_noise, d))]).astype(np.float32)
     return np.ascontiguousarray(X[rng.permutation(n)])

@@ -175,6 +175,32 @@ int cuhc_pairwise_distances_noalloc(const float *devicePointsA, int numPointsA,
                                     int metricId, float metricParam, float *deviceDistances,
                                     void *stream);
 
+/* Audit of the tensor-core screen (no counterpart in the reference; a test
+ * and measurement hook, off by default): with on = 1, every pair of every
+ * screened tile is also compared with the reference FP32 squared distance s
+ * and an FP64 recomputation. Results never change; audited passes are
+ * slower. */
+int cuhc_set_screen_audit(int on);
+
+/* Audit results of the current device since the last call, decoded into the
+ * first `count` of: pairs audited; pairs whose screened value D' exceeded
+ * s + 2^-70 (the screen's guarantee; must be 0); the smallest slack
+ * (s - D') / (e (|x|^2 + |y|^2)) with x, y the centred coordinates and e the
+ * screen's margin; the largest (s64 - D') / (|x|^2 + |y|^2); the largest
+ * s64 - D'; the largest |s - s64| and |s - s64| / s64. NaN where nothing was
+ * observed. Resets them. */
+int cuhc_screen_audit(double *out, int count);
+
+/* Self-test of the bounded device waits (no counterpart in the reference;
+ * the reference's cooperative chain spins without a limit, nn_chain.cuh:84-170).
+ * kind 0: the NN-chain kernel's grid barrier over a 4-block cooperative
+ * launch; kind 1: the pass kernels' mbarrier wait. missing != 0 leaves one
+ * arrival out (a block that returns first; an arrival never made), so every
+ * waiter must give up after about limitMicroseconds (1 .. 1,000,000) and the
+ * call returns CUHC_ERROR_TIMEOUT with the context still usable; missing == 0
+ * must return 0. */
+int cuhc_wait_selftest(int kind, int missing, int limitMicroseconds);
+
 /* Number of this library's own kernel launches since load. */
 unsigned long long cuhc_launch_count(void);
 

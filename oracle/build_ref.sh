@@ -11,9 +11,11 @@
 # as the reference's CMake Release build (CMakeLists.txt:15-41): C++17, -O3,
 # -lineinfo, position-independent shared library.
 #
-# Usage: oracle/build_ref.sh [reference root, default /root/reference]
+# Usage: oracle/build_ref.sh [reference root]
+# The root defaults to $CUHC_REFERENCE_ROOT, else /root/reference (where this
+# recipe finds the read-only checkout of the reference).
 set -euo pipefail
-REF="${1:-/root/reference}"
+REF="${1:-${CUHC_REFERENCE_ROOT:-/root/reference}}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
 if [ ! -f "$REF/src/capi.cu" ]; then

@@ -79,8 +79,7 @@ def gpu():
             out[f"{name}/Z"], out[f"{name}/core"] = Z, core
         elif spec["kind"] == "ward":
             out[f"{name}/Z"] = O.reference_linkage(X, "ward", "rnn", pruning="never")
-    target = ROOT / "gpurun_out" / "reference_gpu.npz"
-    target.parent.mkdir(exist_ok=True)
+    target = ROOT / "tests" / "golden" / "reference_gpu.npz"
     np.savez_compressed(target, **out)
     print(f"wrote {len(out)} arrays to {target}")
 

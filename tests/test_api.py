@@ -37,8 +37,8 @@ def huge_spread(n=200):
     (lambda: C.AgglomerativeClustering(linkage="ward", algorithm="mst").fit(blobs(20)),
      "supports linkage"),
     (lambda: C.AgglomerativeClustering(n_clusters=None).fit(blobs(20)), "Exactly one"),
-    (lambda: C.AgglomerativeClustering(n_clusters=0).fit(blobs(20)), "positive integer"),
-    (lambda: C.AgglomerativeClustering(n_clusters=30).fit(blobs(20)), "Cannot extract"),
+    (lambda: C.AgglomerativeClustering(n_clusters=0).fit(blobs(20)), "integer >= 1"),
+    (lambda: C.AgglomerativeClustering(n_clusters=30).fit(blobs(20)), "exceeds the 20 samples"),
     (lambda: C.fcluster(np.zeros((3, 4)), 0), "t >= 1"),
     (lambda: C.fcluster(np.zeros((3, 4)), 3, criterion="inconsistent"), "criterion"),
 ])

@@ -49,7 +49,8 @@ def no_alloc(torch, A, B, metric, p=2.0):
     return out.cpu().numpy()
 
 
-@pytest.mark.parametrize("metric, p", [(0, 2.0), (1, 2.0), (2, 2.0), (4, 3.0), (5, 2.0)])
+@pytest.mark.parametrize("metric, p", [(0, 2.0), (1, 2.0), (2, 2.0), (3, 2.0), (4, 3.0),
+                                      (5, 2.0)])
 def test_matches_regular_entry_point_twice(metric, p):
     torch = pytest.importorskip("torch")
     rng = np.random.default_rng(metric)
