@@ -41,6 +41,73 @@ def as_points(array, name):
     return points
 
 
+class DevicePoints:
+    """A float32, C-contiguous, 2-D array already in CUDA memory, seen
+    through __cuda_array_interface__ (CuPy, PyTorch, Numba) or DLPack: the
+    device entry points read it in place, with no host copy."""
+
+    def __init__(self, owner, pointer, shape):
+        self.owner, self.pointer, self.shape = owner, pointer, shape
+
+
+def device_points(array, name):
+    """DevicePoints for a CUDA array, None for anything else (host arrays).
+
+    The array must be float32, C-contiguous, 2-D and non-empty; the work that
+    produced it must be complete (PyTorch's and CuPy's current streams are
+    synchronized here). NaN / infinity and the float32 range are not checked
+    on the host for device arrays: non-finite distances still surface as the
+    library's non-finite / disconnected errors."""
+    owner = array
+    cai = getattr(array, "__cuda_array_interface__", None)
+    if cai is None and hasattr(array, "__dlpack__") and hasattr(array, "__dlpack_device__"):
+        kind, _ = array.__dlpack_device__()
+        if kind != 2:  # kDLCUDA
+            return None
+        import torch  # noqa: PLC0415 - DLPack objects are imported through torch
+        owner = torch.utils.dlpack.from_dlpack(array)
+        cai = owner.__cuda_array_interface__
+    if cai is None:
+        return None
+    shape = tuple(int(x) for x in cai["shape"])
+    if cai.get("typestr") != "<f4":
+        raise ValueError(f"{name} on the GPU must be float32, got {cai.get('typestr')!r}")
+    if len(shape) != 2:
+        raise ValueError(f"{name} must be 2D (points x features); its shape is {shape}")
+    if shape[0] == 0 or shape[1] == 0:
+        raise ValueError(f"{name} must be non-empty; its shape is {shape}")
+    strides = cai.get("strides")
+    if strides is not None and tuple(strides) != (4 * shape[1], 4):
+        raise ValueError(f"{name} on the GPU must be C-contiguous")
+    _synchronize_producer(owner)
+    return DevicePoints(owner, int(cai["data"][0]), shape)
+
+
+def _synchronize_producer(owner):
+    module = type(owner).__module__.split(".")[0]
+    if module == "torch":
+        import torch  # noqa: PLC0415
+        torch.cuda.current_stream(owner.device).synchronize()
+    elif module == "cupy":
+        import cupy  # noqa: PLC0415
+        cupy.cuda.get_current_stream().synchronize()
+
+
+def _empty_like_device(owner, shape):
+    """A float32 device array of `shape` from the input's own framework."""
+    module = type(owner).__module__.split(".")[0]
+    if module == "torch":
+        import torch  # noqa: PLC0415
+        out = torch.empty(shape, dtype=torch.float32, device=owner.device)
+        return out, out.data_ptr()
+    if module == "cupy":
+        import cupy  # noqa: PLC0415
+        out = cupy.empty(shape, dtype=cupy.float32)
+        return out, out.data.ptr
+    raise ValueError("pairwise_distances on device arrays needs PyTorch or CuPy arrays "
+                     "(the output is allocated by the input's framework)")
+
+
 def _distance_bound(spread, magnitude, metric, p):
     """Largest value any accumulated float32 distance of the data can take."""
     kind = METRIC_IDS[metric]
@@ -79,6 +146,9 @@ def pairwise_distances(X, Y=None, metric="euclidean", p=2.0):
     metrics, bad shapes, NaN/inf input or distances beyond float32.
     """
     validate_metric(metric, p)
+    X_dev = device_points(X, "X")
+    if X_dev is not None:
+        return _pairwise_on_device(X_dev, Y, metric, p)
     X = as_points(X, "X")
     if Y is not None:
         Y = as_points(Y, "Y")
@@ -91,4 +161,21 @@ def pairwise_distances(X, Y=None, metric="euclidean", p=2.0):
     _lib.check(_lib.lib.cuhc_pairwise_distances(
         _lib.float_ptr(X), X.shape[0], None if Y is None else _lib.float_ptr(Y), rows_b,
         X.shape[1], METRIC_IDS[metric], float(p), _lib.float_ptr(out)))
+    return out
+
+
+def _pairwise_on_device(X, Y, metric, p):
+    """pairwise_distances of a device array: the output is a device array of
+    the input's framework (PyTorch or CuPy)."""
+    Y_dev = None if Y is None else device_points(Y, "Y")
+    if Y is not None and Y_dev is None:
+        raise ValueError("X and Y must both be device arrays or both host arrays")
+    if Y_dev is not None and Y_dev.shape[1] != X.shape[1]:
+        raise ValueError("X and Y must have the same number of features, got "
+                         f"{X.shape[1]} and {Y_dev.shape[1]}")
+    rows_b = X.shape[0] if Y_dev is None else Y_dev.shape[0]
+    out, out_ptr = _empty_like_device(X.owner, (X.shape[0], rows_b))
+    _lib.check(_lib.lib.cuhc_pairwise_distances_device(
+        X.pointer, X.shape[0], None if Y_dev is None else Y_dev.pointer, rows_b, X.shape[1],
+        METRIC_IDS[metric], float(p), out_ptr))
     return out

@@ -12,7 +12,7 @@ import numbers
 import numpy as np
 from sklearn.base import BaseEstimator, ClusterMixin
 
-from ._distances import as_points
+from ._distances import as_points, device_points
 from ._linkage import LINKAGE_IDS, cut_tree, linkage, resolve_algorithm, validate_linkage
 
 
@@ -64,14 +64,15 @@ class AgglomerativeClustering(ClusterMixin, BaseEstimator):
                 raise ValueError(f"n_clusters={self.n_clusters} exceeds the {n_samples} samples")
 
     def fit(self, X, y=None):
-        points = as_points(X, "X")
-        n_samples = points.shape[0]
+        device = device_points(X, "X")  # GPU arrays are read in place
+        points = X if device is not None else as_points(X, "X")
+        n_samples, n_features = device.shape if device is not None else points.shape
         self._validate(n_samples)
         tree = linkage(points, method=self.linkage, metric=self.metric, algorithm=self.algorithm)
         heights = tree[:, 2]
         clusters = self._flat_cut_size(heights, n_samples)
         self.n_leaves_ = n_samples
-        self.n_features_in_ = points.shape[1]
+        self.n_features_in_ = n_features
         self.n_connected_components_ = 1  # every tree here joins all points
         self.children_ = tree[:, :2].astype(np.intp)
         self.n_clusters_ = clusters

@@ -6,7 +6,8 @@ import numbers
 import numpy as np
 
 from . import _lib
-from ._distances import METRIC_IDS, as_points, check_distance_range, validate_metric
+from ._distances import (METRIC_IDS, as_points, check_distance_range, device_points,
+                         validate_metric)
 
 NOISE = -1
 # Core-distance methods of the C ABI (reference hdbscan.cuh:324).
@@ -17,14 +18,20 @@ def hdbscan_tree(X, min_samples, metric="euclidean", alpha=1.0, p=2.0, core_meth
     """(Z, core): the (n-1, 4) single-linkage tree of the mutual reachability
     distance max(core_a, core_b, d(a, b) / alpha) and the core distances
     (distance to the min_samples-th nearest point, the point itself first)."""
-    X = as_points(X, "X")
-    check_distance_range(X, metric, p, scale=1.0 / alpha)
-    n = X.shape[0]
+    X_dev = device_points(X, "X")
+    if X_dev is None:
+        X = as_points(X, "X")
+        check_distance_range(X, metric, p, scale=1.0 / alpha)
+    n, d = X.shape if X_dev is None else X_dev.shape
     tree = np.empty((max(n - 1, 0), 4), dtype=np.float64)
     core = np.empty(n, dtype=np.float32)
-    _lib.check(_lib.lib.cuhc_hdbscan_tree(
-        _lib.float_ptr(X), n, X.shape[1], METRIC_IDS[metric], float(p), int(min_samples),
-        float(alpha), CORE_METHOD_IDS[core_method], _lib.double_ptr(tree), _lib.float_ptr(core)))
+    args = (n, d, METRIC_IDS[metric], float(p), int(min_samples), float(alpha),
+            CORE_METHOD_IDS[core_method], _lib.double_ptr(tree), _lib.float_ptr(core))
+    if X_dev is not None:
+        # Points already in GPU memory (CuPy, PyTorch, DLPack): read in place.
+        _lib.check(_lib.lib.cuhc_hdbscan_tree_device(X_dev.pointer, *args))
+    else:
+        _lib.check(_lib.lib.cuhc_hdbscan_tree(_lib.float_ptr(X), *args))
     return tree, core
 
 
@@ -122,8 +129,10 @@ class HDBSCAN(ClusterMixin, BaseEstimator):
 
     def fit(self, X, y=None):
         self._check_params()
-        X = as_points(X, "X")
-        n = X.shape[0]
+        X_dev = device_points(X, "X")
+        if X_dev is None:
+            X = as_points(X, "X")
+        n, d = X.shape if X_dev is None else X_dev.shape
         k = self.min_cluster_size if self.min_samples is None else self.min_samples
         if k > n:
             raise ValueError(f"min_samples ({k}) must be at most the number of samples ({n})")
@@ -133,7 +142,7 @@ class HDBSCAN(ClusterMixin, BaseEstimator):
             self.cluster_selection_epsilon, self.max_cluster_size)
         self._single_linkage_tree_ = Z
         self.core_distances_ = core
-        self.n_features_in_ = X.shape[1]
+        self.n_features_in_ = d
         return self
 
     def fit_predict(self, X, y=None):

@@ -48,6 +48,9 @@ lib.cuhc_linkage_device.argtypes = [ctypes.c_void_p, _int, _int, _int, _float, _
 lib.cuhc_hdbscan_tree_device.restype = _int
 lib.cuhc_hdbscan_tree_device.argtypes = [ctypes.c_void_p, _int, _int, _int, _float, _int, _float,
                                          _int, _f64, _f32]
+lib.cuhc_pairwise_distances_device.restype = _int
+lib.cuhc_pairwise_distances_device.argtypes = [ctypes.c_void_p, _int, ctypes.c_void_p, _int, _int,
+                                               _int, _float, ctypes.c_void_p]
 lib.cuhc_pass_stats.restype = _int
 lib.cuhc_pass_stats.argtypes = [_u64, _int]
 

@@ -9,7 +9,8 @@ fcluster / cut_tree semantics (:152-216).
 import numpy as np
 
 from . import _lib
-from ._distances import METRIC_IDS, as_points, check_distance_range, validate_metric
+from ._distances import (METRIC_IDS, as_points, check_distance_range, device_points,
+                         validate_metric)
 
 LINKAGE_IDS = {"single": 0, "complete": 1, "average": 2, "ward": 3}
 ALGORITHM_IDS = {"dense": 0, "mst": 1, "nn_chain": 2, "rnn": 3}
@@ -51,17 +52,28 @@ def linkage(X, method="single", metric="euclidean", p=2.0, *, algorithm="auto"):
     validate_linkage(method, metric)
     resolve_algorithm(algorithm, method)
     validate_metric(metric, p)
-    X = as_points(X, "X")
-    n = X.shape[0]
-    # Ward heights grow with cluster size: 2 n_a n_b / (n_a + n_b) <= n.
-    check_distance_range(X, metric, p, scale=n if method == "ward" else 1.0)
     algorithm = resolve_algorithm(algorithm, method)
-    tree = np.empty((max(n - 1, 0), 4), dtype=np.float64)
-    if n == 1:
-        return tree
-    status = _lib.lib.cuhc_linkage(_lib.float_ptr(X), n, X.shape[1], METRIC_IDS[metric], float(p),
-                                   LINKAGE_IDS[method], ALGORITHM_IDS[algorithm],
-                                   _lib.double_ptr(tree))
+    X_dev = device_points(X, "X")
+    if X_dev is not None:
+        # Points already in GPU memory (CuPy, PyTorch, DLPack): read in place.
+        n, d = X_dev.shape
+        tree = np.empty((max(n - 1, 0), 4), dtype=np.float64)
+        if n == 1:
+            return tree
+        status = _lib.lib.cuhc_linkage_device(X_dev.pointer, n, d, METRIC_IDS[metric], float(p),
+                                              LINKAGE_IDS[method], ALGORITHM_IDS[algorithm],
+                                              _lib.double_ptr(tree))
+    else:
+        X = as_points(X, "X")
+        n, d = X.shape
+        # Ward heights grow with cluster size: 2 n_a n_b / (n_a + n_b) <= n.
+        check_distance_range(X, metric, p, scale=n if method == "ward" else 1.0)
+        tree = np.empty((max(n - 1, 0), 4), dtype=np.float64)
+        if n == 1:
+            return tree
+        status = _lib.lib.cuhc_linkage(_lib.float_ptr(X), n, d, METRIC_IDS[metric], float(p),
+                                       LINKAGE_IDS[method], ALGORITHM_IDS[algorithm],
+                                       _lib.double_ptr(tree))
     if status == _lib.CUDA_ERROR_OUT_OF_MEMORY and algorithm == "dense":
         hint = " (ward linkage can use algorithm='rnn' instead)" if method == "ward" else ""
         raise MemoryError(f"the dense {n} x {n} distance matrix needs {4 * n * n / 1e9:.1f} GB "

@@ -62,6 +62,51 @@ static __global__ void seedComponentBest(const unsigned long long *__restrict__ 
     atomicMin(&compBest[comp[i]], (unsigned int)(key >> 32));
 }
 
+// Seeds of a round from HDBSCAN's k-NN lists (mutual reachability, alpha
+// 1). A list member j of row i lies within core_i, so the edge (i, j) weighs
+// max(core_i, core_j) (fmaxf is exact: the pass computes the same bits).
+// Per row: seed = the lightest such edge to another component, under the
+// key order (weight, original index), and its weight goes into the
+// component's best (a real edge: a valid bound). The seed is the row's final
+// answer when it weighs core_i and no point outside the list ties the k-th
+// distance: every point outside the list is then farther than core_i, so its
+// edge weighs more than core_i, the least any edge of row i can weigh. Such a
+// row is settled: its answer goes to nearest now and the pass skips it.
+static __global__ void seedFromKnn(const int *__restrict__ knnPos, const int *__restrict__ knnTie,
+                                   int k, const float *__restrict__ core,
+                                   const int *__restrict__ order, const int *__restrict__ comp,
+                                   unsigned long long *__restrict__ seed,
+                                   unsigned long long *__restrict__ nearest,
+                                   unsigned int *__restrict__ compBest, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  if (order[i] < 0) {
+    seed[i] = kEmptyKey;
+    return;
+  }
+  const float ci = core[i];
+  const int c = comp[i];
+  unsigned long long best = kEmptyKey;
+  const int *list = knnPos + (size_t)i * k;
+  for (int e = 0; e < k; ++e) {
+    const int j = list[e];
+    if (j < 0 || j == i || comp[j] == c)
+      continue;
+    const unsigned long long key = packKey(fmaxf(ci, core[j]), (uint32_t)order[j]);
+    best = key < best ? key : best;
+  }
+  if (best == kEmptyKey) {
+    seed[i] = kEmptyKey;
+    return;
+  }
+  atomicMin(&compBest[c], (unsigned int)(best >> 32));
+  const bool settled = keyWeight(best) == ci && knnTie[i] == 0;
+  seed[i] = settled ? (best | kSettledKey) : best;
+  if (settled)
+    nearest[i] = best;
+}
+
 static __global__ void componentKeyPass1(const unsigned long long *__restrict__ nearest,
                                   const int *__restrict__ order, const int *__restrict__ comp,
                                   unsigned long long *__restrict__ compKey, int n) {
@@ -154,7 +199,8 @@ static __global__ void relabel(int *__restrict__ comp, const int *__restrict__ p
 
 template <class Metric, class Weight>
 int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, bool prune,
-               DeviceEdges &edges, PassStats *stats, cudaStream_t stream, RadiusLog *radiusLog) {
+               DeviceEdges &edges, PassStats *stats, cudaStream_t stream, RadiusLog *radiusLog,
+               const KnnLists *knn) {
   using namespace boruvka_detail;
   const int n = index.n;
   StatusChain st;
@@ -210,6 +256,14 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
   p.rootOfTile = index.numInstances > 1 ? index.rootOfTile.get() : nullptr;
 
   const bool screened = useScreen<Metric>(index.d, 0) && index.extentsWithin(kScreenMaxExtent);
+  // Seeds from the k-NN lists (mutual reachability with alpha 1 only: there
+  // a list edge's weight needs no distance).
+  bool seeds = false;
+  if constexpr (std::is_same<Weight, MutualReachWeight>::value)
+    seeds = knn && knn->pos && weight.alpha == 1.0f && index.numInstances == 1;
+  DeviceBuffer<unsigned long long> seed;
+  if (seeds)
+    CUHC_TRY(st, seed.allocate(n, stream));
   int numComponents = n, totalEdges = 0, rounds = 0;
   unsigned long long tilesSoFar = 0;
   int hostCounters[4];
@@ -267,6 +321,15 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
       seedComponentBest<<<blocks(n), 256, 0, stream>>>(nearest.get(), index.rank.get(),
                                                        comp.get(), compBest.get(), n);
       noteLaunch();
+    }
+    if constexpr (std::is_same<Weight, MutualReachWeight>::value) {
+      if (seeds) {
+        seedFromKnn<<<blocks(n), 256, 0, stream>>>(knn->pos, knn->tie, knn->k, weight.value,
+                                                   index.order.get(), comp.get(), seed.get(),
+                                                   nearest.get(), compBest.get(), n);
+        noteLaunch();
+        p.seedKey = seed.get();
+      }
     }
     CUHC_TRY(rs, cudaGetLastError());
     p.singletons = first;
@@ -437,7 +500,8 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
 
 template <class Metric>
 int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, float *core,
-                  PassStats *stats, cudaStream_t stream, const int *coreRank) {
+                  PassStats *stats, cudaStream_t stream, const int *coreRank, int *knnPos,
+                  int *knnTie) {
   StatusChain st;
   DeviceBuffer<unsigned long long> tiles;
   DeviceBuffer<int> error;
@@ -467,6 +531,8 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
   p.core = core;
   p.k = k;
   p.coreRank = coreRank;
+  p.knnPos = knnPos;
+  p.knnTie = knnTie;
   CUHC_TRY(st, index.orderTiles(!index.tileWorkValid));
   p.tileOrder = index.tileOrder.get();
   p.tileWork = index.tileWork.get();
@@ -476,8 +542,8 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
   p.screenAudit = screenAuditWords();
   p.rootOfTile = index.numInstances > 1 ? index.rootOfTile.get() : nullptr;
   {
-    const bool screened =
-        useScreen<Metric>(index.d, k) && index.extentsWithin(kScreenMaxExtent);
+    const bool screened = useScreen<Metric>(index.d, k, knnPos != nullptr) &&
+                          index.extentsWithin(kScreenMaxExtent);
     PassTimer timer(screened ? kTimerScreenKnnPass : kTimerKnnPass, stream);
     if (screened)
       CUHC_TRY(st, (launchScreen<Metric, PlainWeight, true>(p, metric, PlainWeight{}, index.kc,

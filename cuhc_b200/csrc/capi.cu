@@ -38,6 +38,9 @@ constexpr int kMaxPruneFeatures = 256;
 // Largest k whose per-row lists fit in shared memory (128 rows x k floats);
 // larger k uses radix select.
 constexpr int kMaxListK = 256;
+// Largest k whose lists are kept for the Borůvka seeds (values and positions
+// in shared memory).
+constexpr int kMaxKeptListK = 64;
 
 std::atomic<int> gPruneMode{kPruneAuto};
 std::mutex gStatsMutex;
@@ -138,19 +141,36 @@ int hdbscanTree(const float *devPoints, int n, int d, const Metric &m, int minSa
   DeviceBuffer<float> core, coreOrig;
   CUHC_TRY(st, core.allocate(paddedToTiles(n), s));
   PassStats stats;
+  // The k-NN pass also keeps every point's list (positions, boundary tie),
+  // which lets the Borůvka rounds settle most rows without a search; with
+  // alpha 1 only (a list edge's weight then needs no distance) and lists
+  // that fit shared memory twice over.
+  const bool radix = coreMethod == kCoreRadix || minSamples > kMaxListK;
+  const bool keepLists = !radix && alpha == 1.0f && minSamples <= kMaxKeptListK && n > 1;
+  DeviceBuffer<int> knnPos, knnTie;
+  if (keepLists) {
+    CUHC_TRY(st, knnPos.allocate((size_t)n * minSamples, s));
+    CUHC_TRY(st, knnTie.allocate(n, s));
+  }
   // Radix select when asked for, or when the per-row lists would not fit
   // shared memory (the reference's Auto picks radix above k = 64).
-  if (coreMethod == kCoreRadix || minSamples > kMaxListK)
+  if (radix)
     CUHC_TRY(st, coreDistancesRadix<Metric>(index, m, minSamples, core.get(), s));
   else
-    CUHC_TRY(st, coreDistances<Metric>(index, m, minSamples, prune, core.get(), &stats, s));
+    CUHC_TRY(st, coreDistances<Metric>(index, m, minSamples, prune, core.get(), &stats, s,
+                                       nullptr, knnPos.get(), knnTie.get()));
   CUHC_TRY(st, index.updateMinValues(core.get()));
   DeviceEdges edges;
   MutualReachWeight weight;
   weight.value = core.get();
   weight.alpha = alpha;
+  KnnLists lists;
+  lists.pos = knnPos.get();
+  lists.tie = knnTie.get();
+  lists.k = minSamples;
   if (n > 1)
-    CUHC_TRY(st, (boruvkaMst<Metric, MutualReachWeight>(index, m, weight, prune, edges, &stats, s)));
+    CUHC_TRY(st, (boruvkaMst<Metric, MutualReachWeight>(index, m, weight, prune, edges, &stats, s,
+                                                        nullptr, keepLists ? &lists : nullptr)));
   if (hostCore && st.ok()) {
     CUHC_TRY(st, coreOrig.allocate(n, s));
     scatterByOrder<<<(n + 255) / 256, 256, 0, s>>>(core.get(), index.order.get(), coreOrig.get(),
@@ -650,6 +670,22 @@ int cuhc_hdbscan_tree_device(const float *devicePoints, int n, int d, int metric
     st(withMetric(metricId, p, [&](auto m) {
       return hdbscanTree(devicePoints, n, d, m, minSamples, alpha, coreMethod, hostTree, hostCore,
                          ctx.stream);
+    }));
+  return st.code;
+}
+
+int cuhc_pairwise_distances_device(const float *devA, int nA, const float *devB, int nB, int d,
+                                   int metricId, float p, float *devOut) {
+  if (nA <= 0 || nB <= 0 || d <= 0 || (!devB && nB != nA))
+    return kErrorInvalidShape;
+  if (metricId < kEuclidean || metricId > kCosine)
+    return kErrorInvalidMetric;
+  CallContext ctx;
+  StatusChain st;
+  st(ctx.status);
+  if (st.ok())
+    st(withMetric(metricId, p, [&](auto m) {
+      return pairwiseDistances(devA, nA, devB, nB, d, m, devOut, ctx.stream);
     }));
   return st.code;
 }

@@ -169,7 +169,20 @@ struct PassParams {
   // computed (null: not recorded).
   const int *tileOrder;
   unsigned int *tileWork;
+  // Knn mode: per position, the positions of its k list entries in
+  // ascending distance (k ints) and a flag set when a point outside the list
+  // lies at exactly the k-th distance (null: not recorded).
+  int *knnPos;
+  int *knnTie;
+  // Nearest mode: per position an initial best key (a real edge of the row,
+  // kEmptyKey: none); kSettledKey in the index bits marks a key that is
+  // already the row's answer: the row neither searches nor writes (null:
+  // no seeds).
+  const unsigned long long *seedKey;
 };
+
+// Index bit of a seed key whose row is settled (indices stay below 2^30).
+constexpr unsigned long long kSettledKey = 1ull << 31;
 
 // Lower bound of every distance between the row tile box (shared memory)
 // and a node box, by warp 0 (lanes split the features).

@@ -29,16 +29,16 @@ int pairwiseDistances(const float *A, int nA, const float *B, int nB, int d, con
 #define CUHC_INSTANTIATE_MST(M)                                                                    \
   template int cuhc::boruvkaMst<M, cuhc::PlainWeight>(                                             \
       cuhc::SpatialIndex &, const M &, const cuhc::PlainWeight &, bool, cuhc::DeviceEdges &,       \
-      cuhc::PassStats *, cudaStream_t, cuhc::RadiusLog *);
+      cuhc::PassStats *, cudaStream_t, cuhc::RadiusLog *, const cuhc::KnnLists *);
 
 #define CUHC_INSTANTIATE_MREACH(M)                                                                 \
   template int cuhc::boruvkaMst<M, cuhc::MutualReachWeight>(                                       \
       cuhc::SpatialIndex &, const M &, const cuhc::MutualReachWeight &, bool, cuhc::DeviceEdges &, \
-      cuhc::PassStats *, cudaStream_t, cuhc::RadiusLog *);
+      cuhc::PassStats *, cudaStream_t, cuhc::RadiusLog *, const cuhc::KnnLists *);
 
 #define CUHC_INSTANTIATE_CORE(M)                                                                   \
   template int cuhc::coreDistances<M>(cuhc::SpatialIndex &, const M &, int, bool, float *,         \
-                                      cuhc::PassStats *, cudaStream_t, const int *);               \
+                                      cuhc::PassStats *, cudaStream_t, const int *, int *, int *); \
   template bool cuhc::screenable<M>(cuhc::SpatialIndex &, int);                                    \
   template float cuhc::timeKnnSample<M>(cuhc::SpatialIndex &, const M &, int, bool, int, float *,  \
                                         cudaStream_t);                                             \

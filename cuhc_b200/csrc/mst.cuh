@@ -42,18 +42,33 @@ void treeFromOrderedMerges(const int *u, const int *v, const float *w, int n, do
 bool mergesFormTree(const std::vector<int> &u, const std::vector<int> &v,
                     const std::vector<float> &w, int n);
 
+// HDBSCAN's k-NN lists (a by-product of the core-distance pass), by
+// position: the positions of each point's k nearest points in ascending
+// distance (itself included) and a flag set when a point outside the list
+// lies at exactly the k-th distance.
+struct KnnLists {
+  const int *pos = nullptr;
+  const int *tie = nullptr;
+  int k = 0;
+};
+
 // Borůvka over the points of an index (Metric x Weight instantiations in
 // inst_<metric>_mst.cu and inst_<metric>_mreach.cu). Fills edges with the
 // n-1 MST edges (original indices).
+// With knn (mutual reachability, alpha 1), every round first seeds each row
+// with its lightest list edge to another component and settles the rows
+// whose list edge is provably their answer (boruvka.cuh, seedFromKnn).
 template <class Metric, class Weight>
 int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, bool prune,
                DeviceEdges &edges, PassStats *stats, cudaStream_t stream,
-               RadiusLog *radiusLog = nullptr);
+               RadiusLog *radiusLog = nullptr, const KnnLists *knn = nullptr);
 
-// Exact core distances (k-th nearest, the point itself first) by position.
+// Exact core distances (k-th nearest, the point itself first) by position;
+// with knnPos / knnTie (n x k and n ints) also the k-NN lists (KnnLists).
 template <class Metric>
 int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, float *core,
-                  PassStats *stats, cudaStream_t stream, const int *coreRank = nullptr);
+                  PassStats *stats, cudaStream_t stream, const int *coreRank = nullptr,
+                  int *knnPos = nullptr, int *knnTie = nullptr);
 
 // The same core distances for any 1 <= k <= n by radix select over chunks of
 // the materialised distance matrix (radix.cuh). Bit-identical to

@@ -53,6 +53,7 @@ struct PassState {
   int listTile[kListCap];
   float listLb[kListCap];
   int frontNode[kFrontierCap];
+  int rowTie[kTile]; // knn mode: a point outside the row's list ties its k-th value
   uint64_t bar[2];
   float thrTile;
   int listLen, frontLen, overflow;
@@ -75,7 +76,10 @@ __device__ __forceinline__ void refreshThresholds(const PassParams &p, const Met
   float t = -INFINITY;
   if (tid < kTile) {
     const int pos = firstRow + tid;
-    const bool valid = pos < p.n && p.order[pos] >= 0; // padding slots never search
+    // Padding slots and settled rows never search.
+    const bool valid = pos < p.n && p.order[pos] >= 0 &&
+                       !(!kKnn && p.seedKey && (p.seedKey[pos] & kSettledKey) &&
+                         p.seedKey[pos] != kEmptyKey);
     float thr, filter = -INFINITY;
     if (kKnn) {
       thr = lists[tid * p.k + p.k - 1];
@@ -209,11 +213,61 @@ __device__ __forceinline__ void insertSorted(float *list, int k, float v) {
   list[lo] = v;
 }
 
+// insertSorted that also moves the entries' positions (pos may be null).
+__device__ __forceinline__ void insertSortedPos(float *list, int *pos, int k, float v, int j) {
+  if (!pos) {
+    insertSorted(list, k, v);
+    return;
+  }
+  int lo = 0, hi = k - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (list[mid] > v)
+      hi = mid;
+    else
+      lo = mid + 1;
+  }
+  int i = k - 1;
+  for (; i - 2 >= lo; i -= 2) {
+    const float a = list[i - 1], b = list[i - 2];
+    const int pa = pos[i - 1], pb = pos[i - 2];
+    list[i] = a;
+    list[i - 1] = b;
+    pos[i] = pa;
+    pos[i - 1] = pb;
+  }
+  for (; i > lo; --i) {
+    list[i] = list[i - 1];
+    pos[i] = pos[i - 1];
+  }
+  list[lo] = v;
+  pos[lo] = j;
+}
+
+// Offers value v of position j to a row's k-NN list. Inserts it when it
+// beats the k-th value and keeps `tie` = "some point outside the list lies at
+// exactly the k-th value": an insertion evicts the old k-th, which ties the
+// new k-th when they are equal (a smaller new k-th clears every earlier
+// tie); a value equal to the k-th that stays out ties it. Returns whether v
+// was inserted.
+__device__ __forceinline__ bool knnOffer(float *list, int *pos, int k, float v, int j, int &tie) {
+  const float kth = list[k - 1];
+  if (v < kth) {
+    insertSortedPos(list, pos, k, v, j);
+    tie = (kth < INFINITY && list[k - 1] == kth) ? 1 : 0;
+    return true;
+  }
+  if (v == kth)
+    tie = 1;
+  return false;
+}
+
 template <class Metric>
-__device__ __forceinline__ void knnEpilogue(const Metric &m, const PassState &sh, float *lists,
-                                            int k, typename Metric::Acc (&acc)[8][8],
-                                            int firstRow, int firstCol, int n,
-                                            const int *colOrig, const TileGeom &g) {
+__device__ __forceinline__ void knnEpilogue(const Metric &m, PassState &sh, float *lists,
+                                            int *listPos, int k,
+                                            typename Metric::Acc (&acc)[8][8], int firstRow,
+                                            int firstCol, int n, const int *colOrig,
+                                            const TileGeom &g) {
   const int lane = threadIdx.x & 31;
   const unsigned groupMask = (lane < 16) ? 0x0000ffffu : 0xffff0000u;
 #pragma unroll
@@ -251,7 +305,8 @@ __device__ __forceinline__ void knnEpilogue(const Metric &m, const PassState &sh
         const int colPos = firstCol + g.col(c);
         // The point itself counts as distance 0 (hdbscan.cuh:205-212).
         const float v = colPos == rowPos ? 0.0f : fmaxf(m.finalize(a), 0.0f);
-        insertSorted(list, k, v);
+        knnOffer(list, listPos ? listPos + rowInTile * k : nullptr, k, v, colPos,
+                 sh.rowTie[rowInTile]);
       }
       __syncwarp();
     }
@@ -404,6 +459,7 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
   float *rowLow = (float *)(metaBase + 6 * kTile);
   float *rowHigh = rowLow + p.d;
   float *lists = rowHigh + p.d;
+  int *listPos = (kKnn && p.knnPos) ? reinterpret_cast<int *>(lists + kTile * p.k) : nullptr;
 
   const TileGeom g;
   const int tid = threadIdx.x;
@@ -426,11 +482,20 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
     rowComp[r] = valid ? (p.component ? p.component[pos] : p.order[pos]) : -2;
     rowVal[r] = valid ? w.load(pos) : 0.0f;
   }
-  if (tid < kTile)
-    sh.rowBest[tid] = kEmptyKey;
+  if (tid < kTile) {
+    const int pos = firstRow + tid;
+    const unsigned long long seed =
+        (!kKnn && p.seedKey && pos < p.n) ? p.seedKey[pos] : kEmptyKey;
+    // A settled row keeps its seed as the answer (written before the pass).
+    sh.rowBest[tid] = (seed & kSettledKey) && seed != kEmptyKey ? kEmptyKey : seed;
+    sh.rowTie[tid] = 0;
+  }
   if (kKnn)
-    for (int i = tid; i < kTile * p.k; i += kThreads)
+    for (int i = tid; i < kTile * p.k; i += kThreads) {
       lists[i] = INFINITY;
+      if (listPos)
+        listPos[i] = -1;
+    }
   for (int f = tid; f < p.d; f += kThreads) {
     rowLow[f] = p.nodeLow[(size_t)leaf * p.d + f];
     rowHigh[f] = p.nodeHigh[(size_t)leaf * p.d + f];
@@ -480,7 +545,7 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
         acc[r][c] = m.init();
     accumulateChunk<Metric, KC>(sA, bTile, m, acc, g);
     if (kKnn)
-      knnEpilogue(m, sh, lists, p.k, acc, firstRow, J * kTile, p.n, cm.orig, g);
+      knnEpilogue(m, sh, lists, listPos, p.k, acc, firstRow, J * kTile, p.n, cm.orig, g);
     else
       nearestEpilogue<Metric, Weight>(m, w, sh, cm, acc, rowComp, rowVal, J * kTile, p.n,
                                       useComp, useValue,
@@ -503,7 +568,7 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
     typename Metric::Acc acc[8][8];
     computeTile<Metric, KC>(p.tiled, p.tiled, p.numChunks, I, J, sA, sB[0], m, acc, g);
     if (kKnn)
-      knnEpilogue(m, sh, lists, p.k, acc, firstRow, J * kTile, p.n, meta[0].orig, g);
+      knnEpilogue(m, sh, lists, listPos, p.k, acc, firstRow, J * kTile, p.n, meta[0].orig, g);
     else
       nearestEpilogue<Metric, Weight>(m, w, sh, meta[0], acc, rowComp, rowVal, J * kTile, p.n,
                                       useComp, useValue, maskPass, g, sh.rowBest);
@@ -611,7 +676,14 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
       if (kKnn) {
         const int rank = p.coreRank ? p.coreRank[pos] : p.k;
         p.core[pos] = rank > 0 ? lists[tid * p.k + rank - 1] : 0.0f;
-      } else if (!p.radius || p.radius[pos] >= 0.0f) {
+        if (listPos) {
+          for (int e = 0; e < p.k; ++e)
+            p.knnPos[(size_t)pos * p.k + e] = listPos[tid * p.k + e];
+          p.knnTie[pos] = sh.rowTie[tid];
+        }
+      } else if ((!p.radius || p.radius[pos] >= 0.0f) &&
+                 !(p.seedKey && (p.seedKey[pos] & kSettledKey) &&
+                   p.seedKey[pos] != kEmptyKey)) {
         p.nearest[pos] = sh.rowBest[tid];
       }
     }
@@ -630,8 +702,9 @@ __global__ void __launch_bounds__(kThreads, 2) passKernel(PassParams p, Metric m
 template <class Metric, class Weight, bool kKnn>
 int launchPass(const PassParams &p, const Metric &m, const Weight &w, int kc,
                cudaStream_t stream) {
+  const size_t listEntries = kKnn ? (size_t)kTile * p.k * (p.knnPos ? 2 : 1) : 0;
   const size_t dynBytes = (size_t)3 * kc * kTile * sizeof(float) + 6 * kTile * sizeof(int) +
-                          (size_t)(2 * p.d + (kKnn ? kTile * p.k : 0)) * sizeof(float);
+                          (2 * (size_t)p.d + listEntries) * sizeof(float);
   // Bulk copies need 16-byte aligned sources (pool allocations are 256-byte
   // aligned; refuse anything else rather than fault).
   auto misaligned = [](const void *ptr) { return ((uintptr_t)ptr & 15) != 0; };

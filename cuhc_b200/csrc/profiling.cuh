@@ -36,9 +36,10 @@ unsigned long long *screenCounters();
 // screen's guarantee broken; must stay 0), then minima / maxima stored as
 // order-preserving float bits (min: complemented) of
 //   slack      (s - D') / (e (|x|^2 + |y|^2)), x, y the centred coordinates
-//              and e the screen's margin; >= 0 is the guarantee, and the
-//              margin is twice the modelled error, so about 0.5 or more
-//              means the error model holds with room to spare;
+//              and e the screen's margin, over the pairs whose margin
+//              e (|x|^2 + |y|^2) exceeds the absolute 2^-70; >= 0 is the
+//              guarantee, and the margin is twice the modelled error, so
+//              about 0.5 or more means the error model holds with room;
 //   boundGap   (s64 - D') / (|x|^2 + |y|^2): how far below the exact value
 //              the screened bound sits, relative to the norms;
 //   boundAbs   s64 - D';

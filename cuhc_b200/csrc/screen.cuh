@@ -93,7 +93,10 @@ template <int KC> struct ScreenLayout {
   static constexpr size_t opB = opA + (size_t)kTile * kPad;
   static constexpr size_t box = opB + 2 * (size_t)kTile * kPad; // low, high, centre (KC each)
   static constexpr size_t lists = box + 3 * KC;
-  static size_t bytes(int k) { return (lists + (size_t)kTile * k) * sizeof(float); }
+  // k-NN lists: k values per row, then (when recorded) k positions per row.
+  static size_t bytes(int k, bool positions) {
+    return (lists + (size_t)kTile * k * (positions ? 2 : 1)) * sizeof(float);
+  }
 };
 
 struct ScreenSync {
@@ -243,7 +246,10 @@ __device__ __noinline__ void auditTile(unsigned long long *words, uint32_t taddr
       if (dp > s + 0x1p-70)
         ++violations;
       const double norms = ni + nj;
-      if (norms > 0.0) {
+      // The relative margin is the guarantee where it exceeds the absolute
+      // 2^-70 (below it, flushed and underflowed products are covered by
+      // the absolute term alone, and D' <= s + 2^-70 is what counts).
+      if ((double)margin * norms > 0x1p-70) {
         minSlack = fminf(minSlack, (float)((s - dp) / ((double)margin * norms)));
         maxGap = fmaxf(maxGap, (float)((s64 - dp) / norms));
       }
@@ -298,6 +304,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   float *opA = dyn + L::opA, *opB = dyn + L::opB;
   float *rowLow = dyn + L::box, *rowHigh = rowLow + KC, *centre = rowHigh + KC;
   float *lists = dyn + L::lists;
+  int *listPos = (kKnn && p.knnPos) ? reinterpret_cast<int *>(lists + kTile * p.k) : nullptr;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool consumer = tid < kTile;
@@ -318,11 +325,20 @@ __global__ void __launch_bounds__(kThreads, 2)
   const bool myValid = consumer && myPos < p.n && p.order[myPos] >= 0; // not a padding slot
   const int myComp = myValid ? (p.component ? p.component[myPos] : p.order[myPos]) : -2;
   const float myVal = myValid ? w.load(myPos) : 0.0f;
-  unsigned int *compSlot = (!kKnn && myValid && p.compBest) ? p.compBest + myComp : nullptr;
+  // A seed is a real edge of the row; a settled seed is its answer already
+  // (written before the pass): the row neither searches nor writes.
+  const unsigned long long mySeed =
+      (!kKnn && myValid && p.seedKey) ? p.seedKey[myPos] : kEmptyKey;
+  const bool settled = mySeed != kEmptyKey && (mySeed & kSettledKey) != 0;
+  const bool mySearch = myValid && !settled;
+  unsigned int *compSlot = (!kKnn && mySearch && p.compBest) ? p.compBest + myComp : nullptr;
 
   if (kKnn)
-    for (int i = tid; i < kTile * p.k; i += kThreads)
+    for (int i = tid; i < kTile * p.k; i += kThreads) {
       lists[i] = INFINITY;
+      if (listPos)
+        listPos[i] = -1;
+    }
   for (int f = tid; f < KC; f += kThreads) {
     const bool real = f < p.d;
     const float lo = real ? p.nodeLow[(size_t)leaf * p.d + f] : 0.0f;
@@ -339,7 +355,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   const bool wantOneHot = !kKnn && useComp && !p.singletons;
   int *rowComps = metaBase; // ring slot 0 is free until the first copy
   if (consumer && wantOneHot)
-    rowComps[myRow] = myValid ? myComp : -1;
+    rowComps[myRow] = mySearch ? myComp : -1;
   if (tid == 0) {
     // Arrival counts: rawFull takes the control's expect-tx (or sentinel)
     // arrival, mmaFull the MMA commit + the control's release of slotTile,
@@ -391,11 +407,11 @@ __global__ void __launch_bounds__(kThreads, 2)
   const uint32_t tmem = ss.tmemBase;
   const bool oneHot = ss.oneHot != 0;
   if (consumer) {
-    buildRowOperand<KC>(sA, centre, scale, myRow, myValid, myComp, ss, opA);
+    buildRowOperand<KC>(sA, centre, scale, myRow, mySearch, myComp, ss, opA);
 #pragma unroll
     for (int k = 0; k < KC; ++k) {
-      float lo = myValid ? sA[k * kTile + myRow] : INFINITY;
-      float hi = myValid ? sA[k * kTile + myRow] : -INFINITY;
+      float lo = mySearch ? sA[k * kTile + myRow] : INFINITY;
+      float hi = mySearch ? sA[k * kTile + myRow] : -INFINITY;
 #pragma unroll
       for (int off = 16; off > 0; off /= 2) {
         lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, off));
@@ -411,13 +427,14 @@ __global__ void __launch_bounds__(kThreads, 2)
 
   // Row threshold: sets F (the row's filter bound) and returns the row's
   // threshold for the block maximum (-inf for rows that can gain nothing).
-  unsigned long long rowBest = kEmptyKey;
+  unsigned long long rowBest = settled ? kEmptyKey : mySeed;
+  int tie = 0; // k-NN: a point outside the row's list ties its k-th value
   float F = -INFINITY;
   auto refresh = [&](unsigned int cb) -> float {
     float thr;
     if (kKnn) {
       thr = lists[myRow * p.k + p.k - 1];
-      F = myValid ? m.filterBound(thr) : -INFINITY;
+      F = mySearch ? m.filterBound(thr) : -INFINITY;
     } else {
       thr = rowBest == kEmptyKey ? INFINITY : keyWeight(rowBest);
       if (compSlot) {
@@ -427,9 +444,9 @@ __global__ void __launch_bounds__(kThreads, 2)
       }
       // A proposed radius caps the threshold after the component exchange
       // (only real edge weights go into compBest); negative: settled row.
-      if (myValid && p.radius)
+      if (mySearch && p.radius)
         thr = fminf(thr, p.radius[myPos]);
-      F = (myValid && thr >= 0.0f && w.feasible(thr, myVal))
+      F = (mySearch && thr >= 0.0f && w.feasible(thr, myVal))
               ? m.filterBound(w.distBound(thr, myVal))
               : -INFINITY;
     }
@@ -729,7 +746,7 @@ __global__ void __launch_bounds__(kThreads, 2)
           }
           const float mn = fminf(fminf(chunkMin[0], chunkMin[1]), fminf(chunkMin[2], chunkMin[3]));
           float Fs = F + kScreenAbsSlack;
-          const bool want = myValid && mn <= Fs;
+          const bool want = mySearch && mn <= Fs;
           if (__any_sync(0xffffffffu, want)) {
             slowRows += want;
             float v[32];
@@ -764,8 +781,8 @@ __global__ void __launch_bounds__(kThreads, 2)
                 if (kKnn) {
                   const float value =
                       J * kTile + jj == myPos ? 0.0f : fmaxf(m.finalize(acc), 0.0f);
-                  if (value < list[p.k - 1]) {
-                    insertSorted(list, p.k, value);
+                  if (knnOffer(list, listPos ? listPos + myRow * p.k : nullptr, p.k, value,
+                               J * kTile + jj, tie)) {
                     Fs = m.filterBound(list[p.k - 1]) + kScreenAbsSlack;
                     dirty = true;
                   }
@@ -842,7 +859,12 @@ __global__ void __launch_bounds__(kThreads, 2)
     if (kKnn) {
       const int rank = myValid ? (p.coreRank ? p.coreRank[myPos] : p.k) : 0;
       p.core[myPos] = rank > 0 ? lists[myRow * p.k + rank - 1] : 0.0f;
-    } else if (!p.radius || p.radius[myPos] >= 0.0f) {
+      if (listPos) {
+        for (int e = 0; e < p.k; ++e)
+          p.knnPos[(size_t)myPos * p.k + e] = listPos[myRow * p.k + e];
+        p.knnTie[myPos] = tie;
+      }
+    } else if ((!p.radius || p.radius[myPos] >= 0.0f) && !settled) {
       p.nearest[myPos] = rowBest;
     }
   }
@@ -900,20 +922,20 @@ template <> struct ScreenSupport<SqEuclideanMetric> {
 constexpr size_t kMaxBlockShared = 227 * 1024;
 constexpr size_t kScreenMinShared = 80 * 1024;
 
-inline size_t screenDynamicBytes(int d, int k) {
+inline size_t screenDynamicBytes(int d, int k, bool positions = false) {
   size_t bytes;
   switch (chunkWidthFor(d)) {
   case 4:
-    bytes = ScreenLayout<4>::bytes(k);
+    bytes = ScreenLayout<4>::bytes(k, positions);
     break;
   case 8:
-    bytes = ScreenLayout<8>::bytes(k);
+    bytes = ScreenLayout<8>::bytes(k, positions);
     break;
   case 16:
-    bytes = ScreenLayout<16>::bytes(k);
+    bytes = ScreenLayout<16>::bytes(k, positions);
     break;
   default:
-    bytes = ScreenLayout<32>::bytes(k);
+    bytes = ScreenLayout<32>::bytes(k, positions);
     break;
   }
   const size_t fixed = sizeof(PassState) + sizeof(ScreenSync);
@@ -924,10 +946,11 @@ inline size_t screenDynamicBytes(int d, int k) {
 // screened: the metric has a screened form, the features fit one chunk of at
 // most 32, the block's shared memory fits, and screening is not switched off.
 // Callers also check the data's extent (SpatialIndex::screenRangeOk).
-template <class Metric> inline bool useScreen(int d, int k) {
+template <class Metric> inline bool useScreen(int d, int k, bool positions = false) {
   return ScreenSupport<Metric>::value && currentScreenMode() != 2 &&
          chunkWidthFor(d) * numChunksFor(d) <= 32 &&
-         screenDynamicBytes(d, k) + sizeof(PassState) + sizeof(ScreenSync) <= kMaxBlockShared;
+         screenDynamicBytes(d, k, positions) + sizeof(PassState) + sizeof(ScreenSync) <=
+             kMaxBlockShared;
 }
 
 // Launches the screened pass; a negative code when the metric or the
@@ -941,7 +964,7 @@ int launchScreen(const PassParams &p, const Metric &m, const Weight &w, int kc,
     if (p.numChunks != 1 || kc != chunkWidthFor(p.d))
       return kErrorInvalidAlgorithm;
     const float margin = screenMargin(p.d, kc);
-    const size_t dynBytes = screenDynamicBytes(p.d, kKnn ? p.k : 0);
+    const size_t dynBytes = screenDynamicBytes(p.d, kKnn ? p.k : 0, kKnn && p.knnPos);
     auto misaligned = [](const void *ptr) { return ((uintptr_t)ptr & 15) != 0; };
     if (misaligned(p.tiled) || misaligned(p.order) || misaligned(p.component) ||
         misaligned(w.value))

@@ -97,6 +97,13 @@ int cuhc_hdbscan_tree_device(const float *devicePoints, int numPoints, int numFe
                              int metricId, float metricParam, int minSamples, float alpha,
                              int coreMethod, double *tree, float *core);
 
+/* cuhc_pairwise_distances with A, B (NULL means B = A, then numPointsB ==
+ * numPointsA) and the numPointsA x numPointsB output in device memory of the
+ * current device; synchronous. */
+int cuhc_pairwise_distances_device(const float *devicePointsA, int numPointsA,
+                                   const float *devicePointsB, int numPointsB, int numFeatures,
+                                   int metricId, float metricParam, float *deviceDistances);
+
 /* HDBSCAN labels (-1 = noise) and membership probabilities of a (n-1) x 4
  * single-linkage tree (HOST memory), scikit-learn 1.9 extraction semantics.
  * method: 0 excess of mass, 1 leaf; maxClusterSize <= 0 means no limit.
