@@ -542,8 +542,8 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
   p.screenAudit = screenAuditWords();
   p.rootOfTile = index.numInstances > 1 ? index.rootOfTile.get() : nullptr;
   {
-    const bool screened = useScreen<Metric>(index.d, k, knnPos != nullptr) &&
-                          index.extentsWithin(kScreenMaxExtent);
+    const bool screened =
+        useScreen<Metric>(index.d, k) && index.extentsWithin(kScreenMaxExtent);
     PassTimer timer(screened ? kTimerScreenKnnPass : kTimerKnnPass, stream);
     if (screened)
       CUHC_TRY(st, (launchScreen<Metric, PlainWeight, true>(p, metric, PlainWeight{}, index.kc,

@@ -187,61 +187,60 @@ __device__ __forceinline__ void nearestEpilogue(const Metric &m, const Weight &w
   }
 }
 
-__device__ __forceinline__ void insertSorted(float *list, int k, float v) {
-  if (!(v < list[k - 1]))
-    return;
-  // Place: after every entry <= v (binary search; list[k - 1] > v), then the
-  // tail moves up one slot, four independent loads before their stores.
-  int lo = 0, hi = k - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (list[mid] > v)
-      hi = mid;
-    else
-      lo = mid + 1;
-  }
-  int i = k - 1;
-  for (; i - 4 >= lo; i -= 4) {
-    const float a = list[i - 1], b = list[i - 2], c = list[i - 3], d = list[i - 4];
-    list[i] = a;
-    list[i - 1] = b;
-    list[i - 2] = c;
-    list[i - 3] = d;
-  }
-  for (; i > lo; --i)
-    list[i] = list[i - 1];
-  list[lo] = v;
-}
-
-// insertSorted that also moves the entries' positions (pos may be null).
+// Inserts value v of position j into a row's sorted k-NN list (v below the
+// k-th value, which leaves the list); pos (the entries' positions) may be
+// null.
+// Walks down from the end four entries at a time (four independent loads per
+// step): after the first tiles of a search most values that still enter a
+// list land near its end, where this stops after one or two steps. The
+// value goes after every entry <= v.
 __device__ __forceinline__ void insertSortedPos(float *list, int *pos, int k, float v, int j) {
-  if (!pos) {
-    insertSorted(list, k, v);
-    return;
-  }
-  int lo = 0, hi = k - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (list[mid] > v)
-      hi = mid;
-    else
-      lo = mid + 1;
-  }
-  int i = k - 1;
-  for (; i - 2 >= lo; i -= 2) {
-    const float a = list[i - 1], b = list[i - 2];
-    const int pa = pos[i - 1], pb = pos[i - 2];
+  int i = k - 1; // the slot being filled; list[k - 1] > v leaves the list
+  for (; i >= 4; i -= 4) {
+    const float a = list[i - 1], b = list[i - 2], c = list[i - 3], d = list[i - 4];
+    int pa = 0, pb = 0, pc = 0, pd = 0;
+    if (pos) {
+      pa = pos[i - 1];
+      pb = pos[i - 2];
+      pc = pos[i - 3];
+      pd = pos[i - 4];
+    }
+    if (!(a > v))
+      goto place;
     list[i] = a;
+    if (pos)
+      pos[i] = pa;
+    if (!(b > v)) {
+      i -= 1;
+      goto place;
+    }
     list[i - 1] = b;
-    pos[i] = pa;
-    pos[i - 1] = pb;
+    if (pos)
+      pos[i - 1] = pb;
+    if (!(c > v)) {
+      i -= 2;
+      goto place;
+    }
+    list[i - 2] = c;
+    if (pos)
+      pos[i - 2] = pc;
+    if (!(d > v)) {
+      i -= 3;
+      goto place;
+    }
+    list[i - 3] = d;
+    if (pos)
+      pos[i - 3] = pd;
   }
-  for (; i > lo; --i) {
+  for (; i > 0 && list[i - 1] > v; --i) {
     list[i] = list[i - 1];
-    pos[i] = pos[i - 1];
+    if (pos)
+      pos[i] = pos[i - 1];
   }
-  list[lo] = v;
-  pos[lo] = j;
+place:
+  list[i] = v;
+  if (pos)
+    pos[i] = j;
 }
 
 // Offers value v of position j to a row's k-NN list. Inserts it when it

@@ -81,6 +81,68 @@ inline float screenMargin(int d, int kc) {
   return (float)(2.0 * (product + norms + mma + centring + reference));
 }
 
+// A k-NN list entry of the screened pass: value bits << 32 | position, so
+// that one 64-bit move carries both and keys order by value (values are
+// clamped at +0, so their bits order like the floats), then by position. An
+// empty entry holds +inf.
+constexpr unsigned long long kEmptyListKey = 0x7f800000ffffffffull;
+
+__device__ __forceinline__ float listKeyValue(unsigned long long key) {
+  return __uint_as_float((uint32_t)(key >> 32));
+}
+
+// Inserts `key` (its value below the k-th, whose entry leaves the list) into
+// a row's ascending key list, after every entry <= key; walks down from the
+// end four entries at a time, as insertSortedPos does.
+__device__ __forceinline__ void insertListKey(unsigned long long *list, int k,
+                                              unsigned long long key) {
+  int i = k - 1;
+  for (; i >= 4; i -= 4) {
+    const unsigned long long a = list[i - 1], b = list[i - 2], c = list[i - 3], d = list[i - 4];
+    if (!(a > key))
+      goto place;
+    list[i] = a;
+    if (!(b > key)) {
+      i -= 1;
+      goto place;
+    }
+    list[i - 1] = b;
+    if (!(c > key)) {
+      i -= 2;
+      goto place;
+    }
+    list[i - 2] = c;
+    if (!(d > key)) {
+      i -= 3;
+      goto place;
+    }
+    list[i - 3] = d;
+  }
+  for (; i > 0 && list[i - 1] > key; --i)
+    list[i] = list[i - 1];
+place:
+  list[i] = key;
+}
+
+// knnOffer on a key list: inserts value v of position j when it beats the
+// k-th value, keeps the boundary-tie flag the same way, and returns the k-th
+// value afterwards in kth.
+__device__ __forceinline__ bool knnOfferKey(unsigned long long *list, int k, float v, int j,
+                                            int &tie, float &kth) {
+  const float old = listKeyValue(list[k - 1]);
+  kth = old;
+  if (v < old) {
+    const float c = v > 0.0f ? v : 0.0f; // +0 for -0: bits must order like values
+    insertListKey(list, k, ((unsigned long long)__float_as_uint(c) << 32) | (uint32_t)j);
+    kth = listKeyValue(list[k - 1]);
+    tie = (old < INFINITY && kth == old) ? 1 : 0;
+    return true;
+  }
+  if (v == old)
+    tie = 1;
+  return false;
+}
+
 // Dynamic shared memory of a screened block, in floats from the base.
 template <int KC> struct ScreenLayout {
   static constexpr int kPad = screenKPad(KC);
@@ -92,11 +154,9 @@ template <int KC> struct ScreenLayout {
   static constexpr size_t opA = meta + kScreenStages * metaInts;
   static constexpr size_t opB = opA + (size_t)kTile * kPad;
   static constexpr size_t box = opB + 2 * (size_t)kTile * kPad; // low, high, centre (KC each)
-  static constexpr size_t lists = box + 3 * KC;
-  // k-NN lists: k values per row, then (when recorded) k positions per row.
-  static size_t bytes(int k, bool positions) {
-    return (lists + (size_t)kTile * k * (positions ? 2 : 1)) * sizeof(float);
-  }
+  static constexpr size_t lists = box + 3 * KC; // 8-byte aligned: KC is even
+  // k-NN lists: k 64-bit keys per row (value bits << 32 | position).
+  static size_t bytes(int k) { return (lists + (size_t)kTile * k * 2) * sizeof(float); }
 };
 
 struct ScreenSync {
@@ -303,8 +363,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   int *metaBase = reinterpret_cast<int *>(dyn + L::meta);
   float *opA = dyn + L::opA, *opB = dyn + L::opB;
   float *rowLow = dyn + L::box, *rowHigh = rowLow + KC, *centre = rowHigh + KC;
-  float *lists = dyn + L::lists;
-  int *listPos = (kKnn && p.knnPos) ? reinterpret_cast<int *>(lists + kTile * p.k) : nullptr;
+  unsigned long long *lists = reinterpret_cast<unsigned long long *>(dyn + L::lists);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool consumer = tid < kTile;
@@ -335,9 +394,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 
   if (kKnn)
     for (int i = tid; i < kTile * p.k; i += kThreads) {
-      lists[i] = INFINITY;
-      if (listPos)
-        listPos[i] = -1;
+      lists[i] = kEmptyListKey;
     }
   for (int f = tid; f < KC; f += kThreads) {
     const bool real = f < p.d;
@@ -433,7 +490,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   auto refresh = [&](unsigned int cb) -> float {
     float thr;
     if (kKnn) {
-      thr = lists[myRow * p.k + p.k - 1];
+      thr = listKeyValue(lists[myRow * p.k + p.k - 1]);
       F = mySearch ? m.filterBound(thr) : -INFINITY;
     } else {
       thr = rowBest == kEmptyKey ? INFINITY : keyWeight(rowBest);
@@ -629,8 +686,13 @@ __global__ void __launch_bounds__(kThreads, 2)
             issueNext();
         __syncwarp();
         const int entry = ss.rawTile[t % kScreenStages];
-        // The builders finished the column operand of ordinal t.
-        if (ok && entry >= 0)
+        // The builders finished ordinal t: its column operand, or (a
+        // sentinel) their pass through it. Waited for the sentinel too: its
+        // mmaFull arrival below completes that barrier's phase of ordinal t,
+        // and it must not do so before every builder has waited on the phase
+        // of ordinal t - 2 -- a parity wait two phases behind would see its
+        // parity again and wait for a phase that never comes.
+        if (ok)
           ok = screenWait(&ss.opBReady[s], (t >> 1) & 1, ss);
         ok = __shfl_sync(0xffffffffu, ok && entry >= 0, 0);
         if (lane == 0) {
@@ -683,7 +745,7 @@ __global__ void __launch_bounds__(kThreads, 2)
       }
     } else {
       // ---- consumers: warps 0..3, row myRow = tensor-memory lane ----
-      float *list = lists + myRow * p.k;
+      unsigned long long *list = lists + myRow * p.k;
       while (true) {
         const int s = t & 1;
         const bool ok = screenWait(&ss.mmaFull[s], (t >> 1) & 1, ss);
@@ -781,9 +843,9 @@ __global__ void __launch_bounds__(kThreads, 2)
                 if (kKnn) {
                   const float value =
                       J * kTile + jj == myPos ? 0.0f : fmaxf(m.finalize(acc), 0.0f);
-                  if (knnOffer(list, listPos ? listPos + myRow * p.k : nullptr, p.k, value,
-                               J * kTile + jj, tie)) {
-                    Fs = m.filterBound(list[p.k - 1]) + kScreenAbsSlack;
+                  float kth;
+                  if (knnOfferKey(list, p.k, value, J * kTile + jj, tie, kth)) {
+                    Fs = m.filterBound(kth) + kScreenAbsSlack;
                     dirty = true;
                   }
                 } else {
@@ -858,10 +920,10 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (consumer && myPos < p.n) {
     if (kKnn) {
       const int rank = myValid ? (p.coreRank ? p.coreRank[myPos] : p.k) : 0;
-      p.core[myPos] = rank > 0 ? lists[myRow * p.k + rank - 1] : 0.0f;
-      if (listPos) {
+      p.core[myPos] = rank > 0 ? listKeyValue(lists[myRow * p.k + rank - 1]) : 0.0f;
+      if (p.knnPos) {
         for (int e = 0; e < p.k; ++e)
-          p.knnPos[(size_t)myPos * p.k + e] = listPos[myRow * p.k + e];
+          p.knnPos[(size_t)myPos * p.k + e] = (int)(uint32_t)lists[myRow * p.k + e];
         p.knnTie[myPos] = tie;
       }
     } else if ((!p.radius || p.radius[myPos] >= 0.0f) && !settled) {
@@ -922,20 +984,20 @@ template <> struct ScreenSupport<SqEuclideanMetric> {
 constexpr size_t kMaxBlockShared = 227 * 1024;
 constexpr size_t kScreenMinShared = 80 * 1024;
 
-inline size_t screenDynamicBytes(int d, int k, bool positions = false) {
+inline size_t screenDynamicBytes(int d, int k) {
   size_t bytes;
   switch (chunkWidthFor(d)) {
   case 4:
-    bytes = ScreenLayout<4>::bytes(k, positions);
+    bytes = ScreenLayout<4>::bytes(k);
     break;
   case 8:
-    bytes = ScreenLayout<8>::bytes(k, positions);
+    bytes = ScreenLayout<8>::bytes(k);
     break;
   case 16:
-    bytes = ScreenLayout<16>::bytes(k, positions);
+    bytes = ScreenLayout<16>::bytes(k);
     break;
   default:
-    bytes = ScreenLayout<32>::bytes(k, positions);
+    bytes = ScreenLayout<32>::bytes(k);
     break;
   }
   const size_t fixed = sizeof(PassState) + sizeof(ScreenSync);
@@ -946,10 +1008,10 @@ inline size_t screenDynamicBytes(int d, int k, bool positions = false) {
 // screened: the metric has a screened form, the features fit one chunk of at
 // most 32, the block's shared memory fits, and screening is not switched off.
 // Callers also check the data's extent (SpatialIndex::screenRangeOk).
-template <class Metric> inline bool useScreen(int d, int k, bool positions = false) {
+template <class Metric> inline bool useScreen(int d, int k) {
   return ScreenSupport<Metric>::value && currentScreenMode() != 2 &&
          chunkWidthFor(d) * numChunksFor(d) <= 32 &&
-         screenDynamicBytes(d, k, positions) + sizeof(PassState) + sizeof(ScreenSync) <=
+         screenDynamicBytes(d, k) + sizeof(PassState) + sizeof(ScreenSync) <=
              kMaxBlockShared;
 }
 
@@ -964,7 +1026,7 @@ int launchScreen(const PassParams &p, const Metric &m, const Weight &w, int kc,
     if (p.numChunks != 1 || kc != chunkWidthFor(p.d))
       return kErrorInvalidAlgorithm;
     const float margin = screenMargin(p.d, kc);
-    const size_t dynBytes = screenDynamicBytes(p.d, kKnn ? p.k : 0, kKnn && p.knnPos);
+    const size_t dynBytes = screenDynamicBytes(p.d, kKnn ? p.k : 0);
     auto misaligned = [](const void *ptr) { return ((uintptr_t)ptr & 15) != 0; };
     if (misaligned(p.tiled) || misaligned(p.order) || misaligned(p.component) ||
         misaligned(w.value))
