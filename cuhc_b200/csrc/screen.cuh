@@ -762,101 +762,98 @@ __global__ void __launch_bounds__(kThreads, 2)
           const float *cVal = reinterpret_cast<const float *>(cOrig + 2 * kTile);
           const bool mask = maskPass && !oneHot && !(rowPure >= 0 && colPure);
           const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * kTile);
-          // Minimum of D' over each 32-column chunk of the row (own component
-          // excluded when masking): two chunk loads in flight per wait, two
-          // independent chains per chunk.
-          float chunkMin[4];
-          {
-            float part[8];
+          // Each half: two 32-column chunk loads in flight, the row minimum of
+          // D' over them (own component excluded when masking, two chains per
+          // chunk), and -- only when some row of the warp has a value within
+          // its bound -- the candidate bits of both chunks, built from the
+          // same registers (no second read of tensor memory).
+          float Fs = F + kScreenAbsSlack;
+          uint32_t cand[4];
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
-              part[q] = INFINITY;
+          for (int half = 0; half < 2; ++half) {
+            uint32_t a[32], b[32];
+            tmemLoad32Async(taddr + half * 64, a);
+            tmemLoad32Async(taddr + half * 64 + 32, b);
+            tmemWaitLoads(a);
+            tmemHold(b);
+            float pa0 = INFINITY, pa1 = INFINITY, pb0 = INFINITY, pb1 = INFINITY;
+            if (mask) {
 #pragma unroll
-            for (int half = 0; half < 2; ++half) {
-              uint32_t a[32], b[32];
-              tmemLoad32Async(taddr + half * 64, a);
-              tmemLoad32Async(taddr + half * 64 + 32, b);
-              tmemWaitLoads(a);
-              tmemHold(b);
-              if (mask) {
+              for (int q = 0; q < 16; ++q) {
+                const uint32_t *src = q < 8 ? a : b;
+                const int c = (q & 7) * 4;
+                const int4 cc = reinterpret_cast<const int4 *>(cComp)[half * 16 + q];
+                float &part = q < 8 ? ((q & 1) ? pa1 : pa0) : ((q & 1) ? pb1 : pb0);
+                part = min3(part, cc.x != myComp ? __uint_as_float(src[c]) : INFINITY,
+                            cc.y != myComp ? __uint_as_float(src[c + 1]) : INFINITY);
+                part = min3(part, cc.z != myComp ? __uint_as_float(src[c + 2]) : INFINITY,
+                            cc.w != myComp ? __uint_as_float(src[c + 3]) : INFINITY);
+              }
+            } else {
 #pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                  const uint32_t *src = q < 8 ? a : b;
-                  const int c = (q & 7) * 4;
-                  const int chain = 4 * half + (q < 8 ? 0 : 2) + (q & 1);
-                  const int4 cc = reinterpret_cast<const int4 *>(cComp)[half * 16 + q];
-                  part[chain] = min3(part[chain],
-                                     cc.x != myComp ? __uint_as_float(src[c]) : INFINITY,
-                                     cc.y != myComp ? __uint_as_float(src[c + 1]) : INFINITY);
-                  part[chain] = min3(part[chain],
-                                     cc.z != myComp ? __uint_as_float(src[c + 2]) : INFINITY,
-                                     cc.w != myComp ? __uint_as_float(src[c + 3]) : INFINITY);
-                }
-              } else {
-#pragma unroll
-                for (int c = 0; c < 32; c += 2) {
-                  const int chain = 4 * half + ((c >> 1) & 1);
-                  part[chain] = min3(part[chain], __uint_as_float(a[c]), __uint_as_float(a[c + 1]));
-                  part[chain + 2] =
-                      min3(part[chain + 2], __uint_as_float(b[c]), __uint_as_float(b[c + 1]));
-                }
+              for (int c = 0; c < 32; c += 4) {
+                pa0 = min3(pa0, __uint_as_float(a[c]), __uint_as_float(a[c + 1]));
+                pa1 = min3(pa1, __uint_as_float(a[c + 2]), __uint_as_float(a[c + 3]));
+                pb0 = min3(pb0, __uint_as_float(b[c]), __uint_as_float(b[c + 1]));
+                pb1 = min3(pb1, __uint_as_float(b[c + 2]), __uint_as_float(b[c + 3]));
               }
             }
+            const bool wantA = mySearch && fminf(pa0, pa1) <= Fs;
+            const bool wantB = mySearch && fminf(pb0, pb1) <= Fs;
+            uint32_t ca = 0, cb = 0;
+            if (__any_sync(0xffffffffu, wantA || wantB)) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-              chunkMin[q] = fminf(part[2 * q], part[2 * q + 1]);
+              for (int c = 0; c < 32; ++c) {
+                ca |= (__uint_as_float(a[c]) <= Fs ? 1u : 0u) << c;
+                cb |= (__uint_as_float(b[c]) <= Fs ? 1u : 0u) << c;
+              }
+              ca = wantA ? ca : 0u;
+              cb = wantB ? cb : 0u;
+            }
+            cand[2 * half] = ca;
+            cand[2 * half + 1] = cb;
           }
-          const float mn = fminf(fminf(chunkMin[0], chunkMin[1]), fminf(chunkMin[2], chunkMin[3]));
-          float Fs = F + kScreenAbsSlack;
-          const bool want = mySearch && mn <= Fs;
-          if (__any_sync(0xffffffffu, want)) {
-            slowRows += want;
-            float v[32];
-#pragma unroll 1
-            for (int chunk = 0; chunk < 4; ++chunk) {
-              // Only chunks holding a value within some row's bound are read
-              // again (the load is warp-wide, so the choice is too).
-              const bool wantChunk = want && chunkMin[chunk] <= Fs;
-              if (!__any_sync(0xffffffffu, wantChunk))
+          uint32_t c0 = cand[0], c1 = cand[1], c2 = cand[2], c3 = cand[3];
+          if (__any_sync(0xffffffffu, (c0 | c1 | c2 | c3) != 0)) {
+            slowRows += (c0 | c1 | c2 | c3) != 0;
+            // The candidates of the row, chunk by chunk: c0 holds the current
+            // chunk (columns base .. base + 31) and the others shift down.
+            int base = 0;
+            while (c0 | c1 | c2 | c3) {
+              if (c0 == 0) {
+                c0 = c1;
+                c1 = c2;
+                c2 = c3;
+                c3 = 0;
+                base += 32;
                 continue;
-              tmemLoad32(taddr + chunk * 32, v);
-              if (!wantChunk)
+              }
+              const int jj = base + __ffs(c0) - 1;
+              c0 &= c0 - 1;
+              if (J * kTile + jj >= p.n || cOrig[jj] < 0)
+                continue; // beyond the points, or a padding slot
+              if (!kKnn && (useComp ? cComp[jj] : cOrig[jj]) == myComp)
                 continue;
-              unsigned candidates = 0;
+              // The reference's exact FP32 distance (zero-padded features add 0).
+              typename Metric::Acc acc = m.init();
 #pragma unroll
-              for (int c = 0; c < 32; ++c)
-                candidates |= (v[c] <= Fs ? 1u : 0u) << c;
-              while (candidates) {
-                const int c = __ffs(candidates) - 1;
-                candidates &= candidates - 1;
-                const int jj = chunk * 32 + c;
-                if (J * kTile + jj >= p.n || cOrig[jj] < 0)
-                  continue; // beyond the points, or a padding slot
-                if (!kKnn && (useComp ? cComp[jj] : cOrig[jj]) == myComp)
-                  continue;
-                // The reference's exact FP32 distance (zero-padded features add 0).
-                typename Metric::Acc acc = m.init();
-#pragma unroll
-                for (int k = 0; k < KC; ++k)
-                  acc = m.accumulate(acc, sA[k * kTile + myRow], raw[k * kTile + jj]);
-                ++rechecks;
-                if (kKnn) {
-                  const float value =
-                      J * kTile + jj == myPos ? 0.0f : fmaxf(m.finalize(acc), 0.0f);
-                  float kth;
-                  if (knnOfferKey(list, p.k, value, J * kTile + jj, tie, kth)) {
-                    Fs = m.filterBound(kth) + kScreenAbsSlack;
+              for (int k = 0; k < KC; ++k)
+                acc = m.accumulate(acc, sA[k * kTile + myRow], raw[k * kTile + jj]);
+              ++rechecks;
+              if (kKnn) {
+                const float value = J * kTile + jj == myPos ? 0.0f : fmaxf(m.finalize(acc), 0.0f);
+                float kth;
+                if (knnOfferKey(list, p.k, value, J * kTile + jj, tie, kth)) {
+                  Fs = m.filterBound(kth) + kScreenAbsSlack;
+                  dirty = true;
+                }
+              } else {
+                const float weight = w.weight(m.finalize(acc), myVal, useValue ? cVal[jj] : 0.0f);
+                if (weight < INFINITY) {
+                  const unsigned long long key = packKey(weight, (uint32_t)cOrig[jj]);
+                  if (key < rowBest) {
+                    rowBest = key;
                     dirty = true;
-                  }
-                } else {
-                  const float weight =
-                      w.weight(m.finalize(acc), myVal, useValue ? cVal[jj] : 0.0f);
-                  if (weight < INFINITY) {
-                    const unsigned long long key = packKey(weight, (uint32_t)cOrig[jj]);
-                    if (key < rowBest) {
-                      rowBest = key;
-                      dirty = true;
-                    }
                   }
                 }
               }
