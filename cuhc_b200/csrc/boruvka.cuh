@@ -46,6 +46,21 @@ static __global__ void fillU32(unsigned int *a, unsigned int v, int n) {
     a[i] = v;
 }
 
+// The screened pass's per-tile metadata of a round: [orig, comp, value] x
+// 128 slots per tile (PassParams::packedMeta); slots past n hold -1, 0, 0.
+static __global__ void packMeta(const int *__restrict__ order, const int *__restrict__ comp,
+                                const float *__restrict__ value, int n, int numTiles,
+                                int *__restrict__ packed) {
+  const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pos >= numTiles * kTile)
+    return;
+  int *tile = packed + (size_t)(pos / kTile) * 3 * kTile + pos % kTile;
+  const bool real = pos < n;
+  tile[0] = real ? order[pos] : -1;
+  tile[kTile] = real ? comp[pos] : 0;
+  tile[2 * kTile] = real && value ? __float_as_int(value[pos]) : 0;
+}
+
 // compBest[comp[i]] <- min over i of last round's edge weights that leave
 // the (new) component of i.
 static __global__ void seedComponentBest(const unsigned long long *__restrict__ nearest,
@@ -256,6 +271,9 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
   p.rootOfTile = index.numInstances > 1 ? index.rootOfTile.get() : nullptr;
 
   const bool screened = useScreen<Metric>(index.d, 0) && index.extentsWithin(kScreenMaxExtent);
+  DeviceBuffer<int> packed;
+  if (screened)
+    CUHC_TRY(st, packed.allocate((size_t)index.numTiles * 3 * kTile, stream));
   // Seeds from the k-NN lists (mutual reachability with alpha 1 only: there
   // a list edge's weight needs no distance).
   bool seeds = false;
@@ -330,6 +348,12 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
         noteLaunch();
         p.seedKey = seed.get();
       }
+    }
+    if (screened) {
+      packMeta<<<blocks(index.numTiles * kTile), 256, 0, stream>>>(
+          index.order.get(), comp.get(), weight.value, n, index.numTiles, packed.get());
+      noteLaunch();
+      p.packedMeta = packed.get();
     }
     CUHC_TRY(rs, cudaGetLastError());
     p.singletons = first;

@@ -179,6 +179,11 @@ struct PassParams {
   // already the row's answer: the row neither searches nor writes (null:
   // no seeds).
   const unsigned long long *seedKey;
+  // Screened passes: per tile, the original indices, component labels and
+  // weight values of its 128 slots packed as [3][128] 32-bit words, so that
+  // one bulk copy stages a column tile's metadata (null: three copies from
+  // order, component and the weight's value array).
+  const int *packedMeta;
 };
 
 // Index bit of a seed key whose row is settled (indices stay below 2^30).

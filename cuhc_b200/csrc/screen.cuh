@@ -28,19 +28,26 @@
 // epilogue masks by component.
 //
 // Pipeline, warp-specialised, one row tile per block:
-//   control warp 7 (one thread): issues the bulk copies of column tiles (raw
-//     coordinates + metadata, a ring of five, two ahead) and the MMAs;
-//   builder warps 4-6: build the column operand of each staged tile (warp 4
-//     two columns per thread) as soon as the MMA that last read its buffer is
+//   producer warp 6: picks the next candidate tile (32 list entries per
+//     step) and lane 0 issues its bulk copies (raw coordinates + metadata)
+//     into a ring of `stages` slots, at most `lead` ordinals beyond the last
+//     one every consumer warp has finished;
+//   MMA warp 7 (one thread): issues the MMA of each tile as soon as its
+//     accumulator and its column operand are ready;
+//   builder warps 4-5: build the column operand of each staged tile (two
+//     columns per thread) as soon as the MMA that last read its buffer is
 //     done;
 //   consumer warps 0-3 (row i = thread = tensor-memory lane): read the
-//     accumulator, take the row minimum, recheck rows with a pair at or below
-//     their filter, refresh the row threshold when it may have changed.
+//     accumulator (row minimum, and candidate bits when some row may gain),
+//     release it, recheck rows with a pair at or below their filter, release
+//     the ring slot, refresh the row threshold when it may have changed.
 // Tensor memory holds two 128 x 128 FP32 accumulators, so the MMAs of tile
-// t + 1 run while the consumers read tile t. mbarriers link the stages:
+// t + 1 run while the consumers read tile t; since a warp releases the
+// accumulator before its exact path, one warp's rechecks delay the others
+// only once it falls behind by the ring's slack. mbarriers link the stages:
 // rawFull (copy landed), opBReady (operand built), mmaFull (MMA done + slot
-// info), tmemEmpty (every consumer warp done with the accumulator, and so
-// with the ring slot two ordinals back). Candidate collection and ordering
+// info), tmemEmpty (every consumer warp has read the accumulator), rawEmpty
+// (every consumer warp done with the ring slot). Candidate collection and ordering
 // are those of passes.cuh, one batch at a time; a sentinel ordinal ends each
 // batch. Every wait is bounded; one that runs out marks the block failed,
 // every later wait gives up at once, and the pass returns kErrorTimeout.
@@ -59,12 +66,20 @@ namespace cuhc {
 // terms and at least 4 component slots, a multiple of the MMA's K step (8).
 __host__ __device__ constexpr int screenKPad(int kc) { return (kc + 8 + 7) / 8 * 8; }
 __host__ __device__ constexpr int screenSlots(int kc) { return screenKPad(kc) - kc - 4; }
-constexpr int kScreenStages = 5; // column tiles staged in shared memory
-constexpr int kScreenAhead = 2;  // copies issued ahead of the tile being built
+// Ring of staged column tiles: `stages` slots (chosen per launch, as many as
+// keep two blocks on an SM, kScreenMinStages .. kScreenMaxStages). The
+// producer issues ordinal o once every consumer warp has finished ordinal
+// o - lead, lead = min(stages - 1, screenLead(KC)): copies run that far ahead
+// of the slowest consumer warp, and a tile is picked against thresholds at
+// most that many tiles old.
+__host__ __device__ constexpr int screenLead(int kc) { return kc <= 8 ? 5 : 4; }
+constexpr int kScreenMinStages = 5;
+constexpr int kScreenMaxStages = 8;
 constexpr int kScreenMaxSlots = 8;
-constexpr int kBuilderWarps = 3; // warps 4..6 build column operands
+constexpr int kBuilderWarps = 2; // warps 4..5 build column operands
 constexpr int kBuilderThreads = 32 * kBuilderWarps;
-constexpr int kControlWarp = 7;  // issues the bulk copies and the MMAs
+constexpr int kProducerWarp = 6; // picks candidate tiles and issues their bulk copies
+constexpr int kMmaWarp = 7;      // issues the MMAs
 constexpr int kFirstPhase = 64;  // tiles of a batch's first phase (then x8 per phase)
 constexpr float kIndicator = 0x1p90f;
 constexpr float kScreenAbsSlack = 0x1p-70f;
@@ -143,31 +158,37 @@ __device__ __forceinline__ bool knnOfferKey(unsigned long long *list, int k, flo
   return false;
 }
 
-// Dynamic shared memory of a screened block, in floats from the base.
+// Dynamic shared memory of a screened block with `stages` ring slots, in
+// floats from the base (every region 16-byte aligned).
 template <int KC> struct ScreenLayout {
   static constexpr int kPad = screenKPad(KC);
   static constexpr size_t rawFloats = (size_t)KC * kTile;
   static constexpr size_t metaInts = 3 * kTile; // orig, comp, value
-  static constexpr size_t sA = 0;
-  static constexpr size_t raw = sA + rawFloats;
-  static constexpr size_t meta = raw + kScreenStages * rawFloats;
-  static constexpr size_t opA = meta + kScreenStages * metaInts;
-  static constexpr size_t opB = opA + (size_t)kTile * kPad;
-  static constexpr size_t box = opB + 2 * (size_t)kTile * kPad; // low, high, centre (KC each)
-  static constexpr size_t lists = box + 3 * KC; // 8-byte aligned: KC is even
-  // k-NN lists: k 64-bit keys per row (value bits << 32 | position).
-  static size_t bytes(int k) { return (lists + (size_t)kTile * k * 2) * sizeof(float); }
+  int stages;
+  __host__ __device__ size_t sA() const { return 0; }
+  __host__ __device__ size_t raw() const { return rawFloats; }
+  __host__ __device__ size_t meta() const { return raw() + stages * rawFloats; }
+  __host__ __device__ size_t opA() const { return meta() + stages * metaInts; }
+  __host__ __device__ size_t opB() const { return opA() + (size_t)kTile * kPad; }
+  // Row box low, high, centre (KC each).
+  __host__ __device__ size_t box() const { return opB() + 2 * (size_t)kTile * kPad; }
+  // k-NN lists: k 64-bit keys per row (value bits << 32 | position); 8-byte
+  // aligned since KC is even.
+  __host__ __device__ size_t lists() const { return box() + 3 * KC; }
+  __host__ __device__ size_t bytes(int k) const {
+    return (lists() + (size_t)kTile * k * 2) * sizeof(float);
+  }
 };
 
 struct ScreenSync {
-  uint64_t rawFull[kScreenStages];
+  uint64_t rawFull[kScreenMaxStages], rawEmpty[kScreenMaxStages];
   uint64_t mmaFull[2], tmemEmpty[2], opBReady[2];
-  int rawTile[kScreenStages]; // column tile (| kPureColumnTile) per ring slot, -1 ends the batch
+  int rawTile[kScreenMaxStages]; // column tile (| kPureColumnTile) per ring slot, -1 ends the batch
   int slotTile[2];            // the same, per accumulator
   float warpThr[4];
   float rowF[kTile]; // each row's filter bound as last refreshed (-inf: gains nothing)
   float groupF[4];   // the largest rowF of each consumer warp's 32 rows
-  int cursor, batchDone; // the control's place in the candidate list at a phase end
+  int cursor, batchDone; // the producer's place in the candidate list at a phase end
   int rowSet[kScreenMaxSlots];
   int rowSetCount, oneHot, failed;
   uint32_t tmemBase;
@@ -348,26 +369,29 @@ __device__ __noinline__ void auditTile(unsigned long long *words, uint32_t taddr
 // on), so that the audit costs the normal kernel nothing.
 template <class Metric, class Weight, int KC, bool kKnn, bool kAudit>
 __global__ void __launch_bounds__(kThreads, 2)
-    screenKernel(PassParams p, Metric m, Weight w, float margin) {
+    screenKernel(PassParams p, Metric m, Weight w, float margin, int stages) {
   using L = ScreenLayout<KC>;
+  const L layout{stages};
   constexpr int kPad = L::kPad;
   constexpr uint32_t kSbo = kPad * 32;
   constexpr int R = screenSlots(KC);
+  const int S = stages;
+  const int lead = min(S - 1, screenLead(KC));
   extern __shared__ __align__(128) float dyn[];
   __shared__ PassState sh;
   __shared__ ScreenSync ss;
   // Bounding box of each consumer warp's valid rows (+inf/-inf when none).
   __shared__ float groupLow[4 * KC], groupHigh[4 * KC];
-  float *sA = dyn + L::sA;
-  float *rawBase = dyn + L::raw;
-  int *metaBase = reinterpret_cast<int *>(dyn + L::meta);
-  float *opA = dyn + L::opA, *opB = dyn + L::opB;
-  float *rowLow = dyn + L::box, *rowHigh = rowLow + KC, *centre = rowHigh + KC;
-  unsigned long long *lists = reinterpret_cast<unsigned long long *>(dyn + L::lists);
+  float *sA = dyn + layout.sA();
+  float *rawBase = dyn + layout.raw();
+  int *metaBase = reinterpret_cast<int *>(dyn + layout.meta());
+  float *opA = dyn + layout.opA(), *opB = dyn + layout.opB();
+  float *rowLow = dyn + layout.box(), *rowHigh = rowLow + KC, *centre = rowHigh + KC;
+  unsigned long long *lists = reinterpret_cast<unsigned long long *>(dyn + layout.lists());
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const bool consumer = tid < kTile;
-  const bool control = tid == kControlWarp * 32;
+  const bool producer = tid == kProducerWarp * 32, mmaThread = tid == kMmaWarp * 32;
   const int I = p.tileOrder ? p.tileOrder[blockIdx.x] : (int)blockIdx.x;
   const int firstRow = I * kTile;
   const int leaf = p.leafOfTile[I];
@@ -414,11 +438,14 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (consumer && wantOneHot)
     rowComps[myRow] = mySearch ? myComp : -1;
   if (tid == 0) {
-    // Arrival counts: rawFull takes the control's expect-tx (or sentinel)
-    // arrival, mmaFull the MMA commit + the control's release of slotTile,
-    // tmemEmpty one per consumer warp, opBReady one per builder warp.
-    for (int s = 0; s < kScreenStages; ++s)
+    // Arrival counts: rawFull takes the producer's expect-tx (or sentinel)
+    // arrival, rawEmpty one per consumer warp, mmaFull the MMA commit + the
+    // MMA thread's release of slotTile, tmemEmpty one per consumer warp,
+    // opBReady one per builder warp.
+    for (int s = 0; s < S; ++s) {
       mbarrierInit(&ss.rawFull[s], 1);
+      mbarrierInit(&ss.rawEmpty[s], 4);
+    }
     for (int s = 0; s < 2; ++s) {
       mbarrierInit(&ss.mmaFull[s], 2);
       mbarrierInit(&ss.tmemEmpty[s], 4);
@@ -533,10 +560,21 @@ __global__ void __launch_bounds__(kThreads, 2)
 
   const uint32_t idesc = umma_idesc_tf32(128, 128);
   const bool maskPass = useComp && !p.singletons;
-  const uint32_t metaBytes = (uint32_t)(kTile * sizeof(int)) * (1 + useComp + useValue);
+  const uint32_t metaBytes =
+      (uint32_t)(kTile * sizeof(int)) * (p.packedMeta ? 3 : 1 + useComp + useValue);
   const uint32_t tileBytes = (uint32_t)(L::rawFloats * sizeof(float));
   int t = 0;      // ordinal of tiles and sentinels through the rings (all threads agree)
-  int issued = 0; // control: ordinals issued
+  int tSlot = 0, tPhase = 0; // t % S and the parity of t / S
+  auto nextOrdinal = [&]() {
+    ++t;
+    if (++tSlot == S) {
+      tSlot = 0;
+      tPhase ^= 1;
+    }
+  };
+  int issued = 0; // producer: ordinals issued
+  int iSlot = 0; // producer: issued % S
+  int qSlot = 0, qPhase = 0; // producer: (issued - lead) % S and its parity
   int lastCommit = -1;
   unsigned long long prefiltered = 0; // candidate tiles no row needed (per thread)
   unsigned long long computed = 0;
@@ -610,7 +648,7 @@ __global__ void __launch_bounds__(kThreads, 2)
       sortCandidates(sh, len);
     __syncthreads();
 
-    // Phases of the batch: the control issues phaseLimit tiles (kFirstPhase,
+    // Phases of the batch: the producer issues phaseLimit tiles (kFirstPhase,
     // then eight times more each phase) and a sentinel; between phases every
     // warp tests the remaining candidates against the rows' current bounds.
     int cursor = 0, phaseLimit = kFirstPhase;
@@ -624,29 +662,44 @@ __global__ void __launch_bounds__(kThreads, 2)
       __syncthreads();
     }
 
-    if (warp == kControlWarp) {
-      // ---- control: lane 0 issues the bulk copies and the MMAs; the whole
-      // warp runs the loop in step and tests candidate tiles row by row ----
-      bool sentinelIssued = false;
+    if (warp == kProducerWarp) {
+      // ---- producer: the warp picks candidate tiles, lane 0 issues the
+      // bulk copies; one ordinal per step until the phase's sentinel ----
       int phaseIssued = 0;
-      // Issues ordinal `issued` into its ring slot: a column tile, or the
-      // batch's sentinel. The slot's previous ordinal (issued - stages) is
-      // done with: at a batch start every ordinal is, and later the caller
-      // has seen every consumer warp release ordinal issued - kScreenAhead
-      // - 2, which each of them does after finishing issued - stages.
-      auto issueNext = [&]() {
-        const int r = issued % kScreenStages;
+      while (true) {
+        // Every consumer warp has finished ordinal issued - lead (and so the
+        // slot's previous ordinal, issued - stages). Every ordinal, sentinels
+        // included, passes through rawEmpty once, so the parity follows the
+        // ordinal, and the slot's next use is not issued yet.
+        if (issued >= lead) {
+          if (!__shfl_sync(0xffffffffu, screenWait(&ss.rawEmpty[qSlot], qPhase, ss), 0))
+            break;
+          if (++qSlot == S) {
+            qSlot = 0;
+            qPhase ^= 1;
+          }
+        }
+        const int r = iSlot;
         int entry = -1;
         if (selfPending) {
           entry = I;
           selfPending = false;
         } else if (phaseIssued < phaseLimit) {
+          // The next entry whose bound is within the block threshold, 32
+          // entries per step (entries the tile test dropped hold +inf).
           const float thr =
               __shfl_sync(0xffffffffu, lane == 0 ? *(volatile float *)&sh.thrTile : 0.0f, 0);
-          while (cursor < len && sh.listLb[cursor] > thr)
-            ++cursor;
-          if (cursor < len)
-            entry = sh.listTile[cursor++];
+          while (cursor < len) {
+            const int c = cursor + lane;
+            const unsigned hit = __ballot_sync(0xffffffffu, c < len && !(sh.listLb[c] > thr));
+            if (hit) {
+              cursor += __ffs(hit) - 1;
+              entry = sh.listTile[cursor++];
+              break;
+            }
+            cursor += 32;
+          }
+          cursor = min(cursor, len);
         }
         if (entry >= 0)
           ++phaseIssued;
@@ -660,41 +713,45 @@ __global__ void __launch_bounds__(kThreads, 2)
             mbarrierArriveExpectTx(&ss.rawFull[r], tileBytes + metaBytes);
             bulkCopyToShared(rawBase + r * L::rawFloats, p.tiled + (size_t)J * L::rawFloats,
                              tileBytes, &ss.rawFull[r]);
-            bulkCopyToShared(meta, p.order + (size_t)J * kTile, kTile * sizeof(int),
-                             &ss.rawFull[r]);
-            if (useComp)
-              bulkCopyToShared(meta + kTile, p.component + (size_t)J * kTile,
-                               kTile * sizeof(int), &ss.rawFull[r]);
-            if (useValue)
-              bulkCopyToShared(meta + 2 * kTile, w.value + (size_t)J * kTile,
-                               kTile * sizeof(float), &ss.rawFull[r]);
+            if (p.packedMeta) {
+              bulkCopyToShared(meta, p.packedMeta + (size_t)J * 3 * kTile, metaBytes,
+                               &ss.rawFull[r]);
+            } else {
+              bulkCopyToShared(meta, p.order + (size_t)J * kTile, kTile * sizeof(int),
+                               &ss.rawFull[r]);
+              if (useComp)
+                bulkCopyToShared(meta + kTile, p.component + (size_t)J * kTile,
+                                 kTile * sizeof(int), &ss.rawFull[r]);
+              if (useValue)
+                bulkCopyToShared(meta + 2 * kTile, w.value + (size_t)J * kTile,
+                                 kTile * sizeof(float), &ss.rawFull[r]);
+            }
           }
         }
-        if (entry < 0)
-          sentinelIssued = true;
         ++issued;
-      };
-      while (!sentinelIssued && issued <= t + kScreenAhead)
-        issueNext();
+        if (++iSlot == S)
+          iSlot = 0;
+        if (entry < 0)
+          break;
+      }
+    } else if (warp == kMmaWarp) {
+      // ---- MMA warp: lane 0 issues the MMAs, the warp runs in step ----
       while (true) {
         const int s = t & 1;
-        // Every consumer warp released ordinal t - 2: accumulator s is free,
-        // and so is the ring slot of ordinal t + kScreenAhead.
+        // Every consumer warp has read ordinal t - 2: accumulator s is free.
         bool ok = __shfl_sync(0xffffffffu, screenWait(&ss.tmemEmpty[s], ((t >> 1) & 1) ^ 1, ss), 0);
-        if (ok)
-          while (!sentinelIssued && issued <= t + kScreenAhead)
-            issueNext();
-        __syncwarp();
-        const int entry = ss.rawTile[t % kScreenStages];
         // The builders finished ordinal t: its column operand, or (a
-        // sentinel) their pass through it. Waited for the sentinel too: its
-        // mmaFull arrival below completes that barrier's phase of ordinal t,
-        // and it must not do so before every builder has waited on the phase
-        // of ordinal t - 2 -- a parity wait two phases behind would see its
-        // parity again and wait for a phase that never comes.
+        // sentinel) their pass through it, after the producer staged it. Waited
+        // for the sentinel too: its mmaFull arrival below completes that
+        // barrier's phase of ordinal t, and it must not do so before every
+        // builder has waited on the phase of ordinal t - 2 -- a parity wait two
+        // phases behind would see its parity again and wait for a phase that
+        // never comes.
         if (ok)
           ok = screenWait(&ss.opBReady[s], (t >> 1) & 1, ss);
-        ok = __shfl_sync(0xffffffffu, ok && entry >= 0, 0);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        const int entry = ok ? ss.rawTile[tSlot] : -1;
+        ok = ok && entry >= 0;
         if (lane == 0) {
           if (ok) {
             tcgenFenceAfter();
@@ -712,34 +769,34 @@ __global__ void __launch_bounds__(kThreads, 2)
             mbarrierArrive(&ss.mmaFull[s], 2);
           }
         }
-        ++t;
+        nextOrdinal();
         if (!ok)
           break;
       }
     } else if (!consumer) {
-      // ---- builders: warps 4..6, column j and (warp 4) column j + 96 ----
+      // ---- builders: warps 4..5, columns j and j + 64 ----
       const int j = tid - kTile;
       while (true) {
         const int s = t & 1;
         // The operand buffer of slot s is free once the MMA of ordinal t - 2
         // has completed (the consumers may still be reading its result).
         bool ok = screenWait(&ss.mmaFull[s], ((t >> 1) & 1) ^ 1, ss);
-        const int r = t % kScreenStages;
-        ok = screenWait(&ss.rawFull[r], (t / kScreenStages) & 1, ss) && ok;
+        const int r = tSlot;
+        ok = screenWait(&ss.rawFull[r], tPhase, ss) && ok;
         const int entry = __shfl_sync(0xffffffffu, ok ? ss.rawTile[r] : -1, 0);
         if (entry >= 0) {
           const float *raw = rawBase + r * L::rawFloats;
           const int *comp = metaBase + r * L::metaInts + kTile;
           float *b = opB + (size_t)s * kTile * kPad;
-          buildColumnOperand<KC>(raw, comp, centre, scale, j, oneHot, ss, b);
-          if (j < kTile - kBuilderThreads)
-            buildColumnOperand<KC>(raw, comp, centre, scale, j + kBuilderThreads, oneHot, ss, b);
+#pragma unroll
+          for (int q = j; q < kTile; q += kBuilderThreads)
+            buildColumnOperand<KC>(raw, comp, centre, scale, q, oneHot, ss, b);
         }
         fenceProxyAsync();
         __syncwarp();
         if (lane == 0)
           mbarrierArrive(&ss.opBReady[s], 1);
-        ++t;
+        nextOrdinal();
         if (entry < 0)
           break;
       }
@@ -751,7 +808,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         const bool ok = screenWait(&ss.mmaFull[s], (t >> 1) & 1, ss);
         tcgenFenceAfter();
         const int entry = __shfl_sync(0xffffffffu, ok ? ss.slotTile[s] : -1, 0);
-        const int r = t % kScreenStages;
+        const int r = tSlot;
         bool thrChanged = false;
         if (entry >= 0) {
           const int J = entry & ~kPureColumnTile;
@@ -813,6 +870,15 @@ __global__ void __launch_bounds__(kThreads, 2)
             cand[2 * half] = ca;
             cand[2 * half + 1] = cb;
           }
+          if (kAudit)
+            auditTile<Metric, KC, kKnn>(p.screenAudit, taddr, m, sA, raw, centre, myRow, myValid,
+                                        myComp, J * kTile, p.n, cOrig, cComp, useComp, margin);
+          // Done with accumulator s: the MMA of ordinal t + 2 may overwrite it
+          // while this warp rechecks.
+          tcgenFenceBefore();
+          __syncwarp();
+          if (lane == 0)
+            mbarrierArrive(&ss.tmemEmpty[s], 1);
           uint32_t c0 = cand[0], c1 = cand[1], c2 = cand[2], c3 = cand[3];
           if (__any_sync(0xffffffffu, (c0 | c1 | c2 | c3) != 0)) {
             slowRows += (c0 | c1 | c2 | c3) != 0;
@@ -859,9 +925,6 @@ __global__ void __launch_bounds__(kThreads, 2)
               }
             }
           }
-          if (kAudit)
-            auditTile<Metric, KC, kKnn>(p.screenAudit, taddr, m, sA, raw, centre, myRow, myValid,
-                                        myComp, J * kTile, p.n, cOrig, cComp, useComp, margin);
           // The row's filter changes only through its own exact path or the
           // component's best (found by other blocks): refresh then, and every
           // eighth tile for the latter.
@@ -871,27 +934,32 @@ __global__ void __launch_bounds__(kThreads, 2)
             thrChanged = true;
           }
           ++computed;
+        } else {
+          tcgenFenceBefore();
+          __syncwarp();
+          if (lane == 0)
+            mbarrierArrive(&ss.tmemEmpty[s], 1);
         }
-        tcgenFenceBefore();
         __syncwarp();
         if (lane == 0) {
-          // This warp is done with accumulator s and ring slot r.
-          mbarrierArrive(&ss.tmemEmpty[s], 1);
+          // This warp is done with ring slot r (every ordinal, sentinels
+          // included, passes through rawEmpty and tmemEmpty once).
+          mbarrierArrive(&ss.rawEmpty[r], 1);
           if (thrChanged)
             *(volatile float *)&sh.thrTile = fmaxf(fmaxf(ss.warpThr[0], ss.warpThr[1]),
                                                    fmaxf(ss.warpThr[2], ss.warpThr[3]));
         }
-        ++t;
+        nextOrdinal();
         if (entry < 0)
           break;
       }
     }
-    if (warp == kControlWarp && lane == 0) {
+    if (warp == kProducerWarp && lane == 0) {
       ss.cursor = cursor;
       ss.batchDone = cursor >= len ? 1 : 0;
     }
     __syncthreads();
-    // The control issued the row tile itself first in the first phase; every
+    // The producer issued the row tile itself first in the first phase; every
     // thread forgets it here so that the loop's exit stays uniform.
     selfPending = false;
     cursor = ss.cursor;
@@ -907,13 +975,13 @@ __global__ void __launch_bounds__(kThreads, 2)
   }
 
   // Nothing may land in shared or tensor memory after the block leaves: on a
-  // failure the control waits (bounded) for its copies and its last MMAs.
-  if (control && ss.failed) {
-    for (int o = t; o < issued; ++o)
-      mbarrierWait(&ss.rawFull[o % kScreenStages], (o / kScreenStages) & 1);
-    if (lastCommit >= 0)
-      mbarrierWait(&ss.mmaFull[lastCommit & 1], (lastCommit >> 1) & 1);
-  }
+  // failure the producer waits (bounded) for its copies (each slot's last
+  // use) and the MMA thread for its last MMAs.
+  if (producer && ss.failed)
+    for (int o = max(0, issued - S); o < issued; ++o)
+      mbarrierWait(&ss.rawFull[o % S], (o / S) & 1);
+  if (mmaThread && ss.failed && lastCommit >= 0)
+    mbarrierWait(&ss.mmaFull[lastCommit & 1], (lastCommit >> 1) & 1);
   if (consumer && myPos < p.n) {
     if (kKnn) {
       const int rank = myValid ? (p.coreRank ? p.coreRank[myPos] : p.k) : 0;
@@ -975,30 +1043,45 @@ template <> struct ScreenSupport<SqEuclideanMetric> {
   static constexpr bool value = true;
 };
 
-// Shared memory a block may use on sm_100 (227 KiB); a screened block keeps
-// at least kScreenMinShared so that at most two share an SM (their tensor
-// memory, 256 columns each, then always fits).
+// Shared memory a block may use on sm_100 (227 KiB), and what each of two
+// blocks on one SM may use (228 KiB per SM, 1 KiB of it reserved per block).
+// A screened block keeps at least kScreenMinShared so that at most two share
+// an SM (their tensor memory, 256 columns each, then always fits).
 constexpr size_t kMaxBlockShared = 227 * 1024;
+constexpr size_t kTwoBlockShared = 113 * 1024;
 constexpr size_t kScreenMinShared = 80 * 1024;
 
-inline size_t screenDynamicBytes(int d, int k) {
-  size_t bytes;
+// Static shared memory of a screened block (an upper bound).
+constexpr size_t kScreenStaticBytes = sizeof(PassState) + sizeof(ScreenSync) + 2 * 4 * 32 * 4;
+
+inline size_t screenLayoutBytes(int d, int k, int stages) {
   switch (chunkWidthFor(d)) {
   case 4:
-    bytes = ScreenLayout<4>::bytes(k);
-    break;
+    return ScreenLayout<4>{stages}.bytes(k);
   case 8:
-    bytes = ScreenLayout<8>::bytes(k);
-    break;
+    return ScreenLayout<8>{stages}.bytes(k);
   case 16:
-    bytes = ScreenLayout<16>::bytes(k);
-    break;
+    return ScreenLayout<16>{stages}.bytes(k);
   default:
-    bytes = ScreenLayout<32>::bytes(k);
-    break;
+    return ScreenLayout<32>{stages}.bytes(k);
   }
-  const size_t fixed = sizeof(PassState) + sizeof(ScreenSync);
-  return bytes + fixed < kScreenMinShared ? kScreenMinShared - fixed : bytes;
+}
+
+// Ring slots of a screened pass: the most that keep two blocks on an SM, or,
+// when not even kScreenMinStages does, the most that fit one block; 0 when
+// nothing fits.
+inline int screenStagesFor(int d, int k) {
+  for (const size_t limit : {kTwoBlockShared, kMaxBlockShared})
+    for (int stages = kScreenMaxStages; stages >= kScreenMinStages; --stages)
+      if (screenLayoutBytes(d, k, stages) + kScreenStaticBytes <= limit)
+        return stages;
+  return 0;
+}
+
+inline size_t screenDynamicBytes(int d, int k, int stages) {
+  const size_t bytes = screenLayoutBytes(d, k, stages);
+  return bytes + kScreenStaticBytes < kScreenMinShared ? kScreenMinShared - kScreenStaticBytes
+                                                       : bytes;
 }
 
 // Whether a pass over d features (k-NN rank k, 0 for a nearest pass) can run
@@ -1007,9 +1090,7 @@ inline size_t screenDynamicBytes(int d, int k) {
 // Callers also check the data's extent (SpatialIndex::screenRangeOk).
 template <class Metric> inline bool useScreen(int d, int k) {
   return ScreenSupport<Metric>::value && currentScreenMode() != 2 &&
-         chunkWidthFor(d) * numChunksFor(d) <= 32 &&
-         screenDynamicBytes(d, k) + sizeof(PassState) + sizeof(ScreenSync) <=
-             kMaxBlockShared;
+         chunkWidthFor(d) * numChunksFor(d) <= 32 && screenStagesFor(d, k) > 0;
 }
 
 // Launches the screened pass; a negative code when the metric or the
@@ -1023,17 +1104,20 @@ int launchScreen(const PassParams &p, const Metric &m, const Weight &w, int kc,
     if (p.numChunks != 1 || kc != chunkWidthFor(p.d))
       return kErrorInvalidAlgorithm;
     const float margin = screenMargin(p.d, kc);
-    const size_t dynBytes = screenDynamicBytes(p.d, kKnn ? p.k : 0);
+    const int stages = screenStagesFor(p.d, kKnn ? p.k : 0);
+    if (stages == 0)
+      return kErrorInvalidAlgorithm;
+    const size_t dynBytes = screenDynamicBytes(p.d, kKnn ? p.k : 0, stages);
     auto misaligned = [](const void *ptr) { return ((uintptr_t)ptr & 15) != 0; };
     if (misaligned(p.tiled) || misaligned(p.order) || misaligned(p.component) ||
-        misaligned(w.value))
+        misaligned(w.value) || misaligned(p.packedMeta))
       return (int)cudaErrorMisalignedAddress;
     auto run = [&](auto kernel) {
       const cudaError_t e =
           cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dynBytes);
       if (e != cudaSuccess)
         return (int)e;
-      kernel<<<p.numTiles, kThreads, dynBytes, stream>>>(p, m, w, margin);
+      kernel<<<p.numTiles, kThreads, dynBytes, stream>>>(p, m, w, margin, stages);
       noteLaunch();
       return (int)cudaGetLastError();
     };
