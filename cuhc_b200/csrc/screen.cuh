@@ -139,25 +139,6 @@ place:
   list[i] = key;
 }
 
-// knnOffer on a key list: inserts value v of position j when it beats the
-// k-th value, keeps the boundary-tie flag the same way, and returns the k-th
-// value afterwards in kth.
-__device__ __forceinline__ bool knnOfferKey(unsigned long long *list, int k, float v, int j,
-                                            int &tie, float &kth) {
-  const float old = listKeyValue(list[k - 1]);
-  kth = old;
-  if (v < old) {
-    const float c = v > 0.0f ? v : 0.0f; // +0 for -0: bits must order like values
-    insertListKey(list, k, ((unsigned long long)__float_as_uint(c) << 32) | (uint32_t)j);
-    kth = listKeyValue(list[k - 1]);
-    tie = (old < INFINITY && kth == old) ? 1 : 0;
-    return true;
-  }
-  if (v == old)
-    tie = 1;
-  return false;
-}
-
 // Dynamic shared memory of a screened block with `stages` ring slots, in
 // floats from the base (every region 16-byte aligned).
 template <int KC> struct ScreenLayout {
@@ -885,6 +866,8 @@ __global__ void __launch_bounds__(kThreads, 2)
             // The candidates of the row, chunk by chunk: c0 holds the current
             // chunk (columns base .. base + 31) and the others shift down.
             int base = 0;
+            // k-NN: the row's k-th value, reloaded only after an insertion.
+            float rowKth = kKnn && mySearch ? listKeyValue(list[p.k - 1]) : 0.0f;
             while (c0 | c1 | c2 | c3) {
               if (c0 == 0) {
                 c0 = c1;
@@ -908,10 +891,23 @@ __global__ void __launch_bounds__(kThreads, 2)
               ++rechecks;
               if (kKnn) {
                 const float value = J * kTile + jj == myPos ? 0.0f : fmaxf(m.finalize(acc), 0.0f);
-                float kth;
-                if (knnOfferKey(list, p.k, value, J * kTile + jj, tie, kth)) {
-                  Fs = m.filterBound(kth) + kScreenAbsSlack;
+                // Offer to the row's list (the k-th value kept in a register):
+                // a value below the k-th enters, and the boundary-tie flag
+                // follows knnOffer (passes.cuh): an insertion evicts the old
+                // k-th, which ties the new k-th when they are equal; a value
+                // equal to the k-th that stays out ties it.
+                if (value < rowKth) {
+                  const float c = value > 0.0f ? value : 0.0f; // +0 for -0: bits order like values
+                  insertListKey(list, p.k,
+                                ((unsigned long long)__float_as_uint(c) << 32) |
+                                    (uint32_t)(J * kTile + jj));
+                  const float old = rowKth;
+                  rowKth = listKeyValue(list[p.k - 1]);
+                  tie = (old < INFINITY && rowKth == old) ? 1 : 0;
+                  Fs = m.filterBound(rowKth) + kScreenAbsSlack;
                   dirty = true;
+                } else if (value == rowKth) {
+                  tie = 1;
                 }
               } else {
                 const float weight = w.weight(m.finalize(acc), myVal, useValue ? cVal[jj] : 0.0f);
