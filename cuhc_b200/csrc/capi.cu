@@ -120,13 +120,12 @@ int singleLinkageMst(const float *devPoints, int n, int d, const Metric &m, doub
   DeviceEdges edges;
   PassStats stats;
   CUHC_TRY(st, (boruvkaMst<Metric, PlainWeight>(index, m, PlainWeight{}, prune, edges, &stats, s)));
-  std::vector<int> u, v;
-  std::vector<float> w;
-  CUHC_TRY(st, sortEdgesToHost(edges, edges.count, s, u, v, w));
-  if (st.ok() && (int)u.size() != n - 1)
+  HostEdges sorted;
+  CUHC_TRY(st, sortEdgesToPinned(edges, edges.count, s, sorted));
+  if (st.ok() && sorted.count != n - 1)
     st(kErrorDisconnected);
   if (st.ok())
-    treeFromOrderedMerges(u, v, w, n, hostTree);
+    treeFromOrderedMerges(sorted.u, sorted.v, sorted.w, n, hostTree);
   addStats(stats);
   return st.code;
 }
@@ -180,13 +179,12 @@ int hdbscanTree(const float *devPoints, int n, int d, const Metric &m, int minSa
                                  cudaMemcpyDeviceToHost, s));
   }
   if (n > 1) {
-    std::vector<int> u, v;
-    std::vector<float> w;
-    CUHC_TRY(st, sortEdgesToHost(edges, edges.count, s, u, v, w));
-    if (st.ok() && (int)u.size() != n - 1)
+    HostEdges sorted;
+    CUHC_TRY(st, sortEdgesToPinned(edges, edges.count, s, sorted));
+    if (st.ok() && sorted.count != n - 1)
       st(kErrorDisconnected);
     if (st.ok())
-      treeFromOrderedMerges(u, v, w, n, hostTree);
+      treeFromOrderedMerges(sorted.u, sorted.v, sorted.w, n, hostTree);
   }
   CUHC_TRY(st, cudaStreamSynchronize(s));
   addStats(stats);

@@ -29,6 +29,16 @@ struct DeviceEdges {
 int sortEdgesToHost(DeviceEdges &edges, int numEdges, cudaStream_t stream, std::vector<int> &u,
                     std::vector<int> &v, std::vector<float> &w);
 
+// Sorted edges in page-locked host memory owned by the calling thread: the
+// buffers grow as needed and are reused by the thread's next call, so a call
+// pays neither page faults nor a staged copy. Valid until that next call.
+struct HostEdges {
+  const int *u = nullptr, *v = nullptr;
+  const float *w = nullptr;
+  int count = 0;
+};
+int sortEdgesToPinned(DeviceEdges &edges, int numEdges, cudaStream_t stream, HostEdges &out);
+
 // scipy linkage rows from merges in tree order (each merge after the merges
 // that made its clusters): union-find names clusters, as the reference's
 // treeFromOrderedMerges (mst.cuh:204-228). Z receives (n-1) x 4 doubles.

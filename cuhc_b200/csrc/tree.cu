@@ -42,25 +42,19 @@ __global__ void iota(int *a, int m) {
 
 } // namespace
 
-int sortEdgesToHost(DeviceEdges &edges, int m, cudaStream_t s, std::vector<int> &u,
-                    std::vector<int> &v, std::vector<float> &w) {
-  u.resize(m);
-  v.resize(m);
-  w.resize(m);
-  if (m == 0)
-    return 0;
+namespace {
+
+// Sorts the edges on the device into uo, vo, wo (device buffers of m).
+int sortEdgesOnDevice(DeviceEdges &edges, int m, cudaStream_t s, DeviceBuffer<int> &uo,
+                      DeviceBuffer<int> &vo, DeviceBuffer<float> &wo) {
   StatusChain st;
-  DeviceBuffer<int> perm, perm2, vKeys, vKeysOut, uo, vo;
-  DeviceBuffer<float> wo;
+  DeviceBuffer<int> perm, perm2, vKeysOut;
   DeviceBuffer<unsigned long long> keys, keysOut;
   CUHC_TRY(st, perm.allocate(m, s));
   CUHC_TRY(st, perm2.allocate(m, s));
   CUHC_TRY(st, vKeysOut.allocate(m, s));
   CUHC_TRY(st, keys.allocate(m, s));
   CUHC_TRY(st, keysOut.allocate(m, s));
-  CUHC_TRY(st, uo.allocate(m, s));
-  CUHC_TRY(st, vo.allocate(m, s));
-  CUHC_TRY(st, wo.allocate(m, s));
   if (!st.ok())
     return st.code;
   const int blocks = (m + 255) / 256;
@@ -83,10 +77,82 @@ int sortEdgesToHost(DeviceEdges &edges, int m, cudaStream_t s, std::vector<int> 
   gatherEdges<<<blocks, 256, 0, s>>>(perm.get(), edges.u.get(), edges.v.get(), edges.w.get(),
                                      uo.get(), vo.get(), wo.get(), m); noteLaunch();
   CUHC_TRY(st, cudaGetLastError());
+  return st.code;
+}
+
+// Page-locked host buffers of the calling thread, grown on demand.
+struct PinnedEdgeBuffers {
+  void *data = nullptr;
+  size_t capacity = 0; // edges
+  ~PinnedEdgeBuffers() {
+    if (data)
+      cudaFreeHost(data);
+  }
+  int reserve(size_t m) {
+    if (m <= capacity)
+      return 0;
+    if (data)
+      cudaFreeHost(data);
+    data = nullptr;
+    capacity = 0;
+    const cudaError_t e = cudaHostAlloc(&data, m * (2 * sizeof(int) + sizeof(float)),
+                                        cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      data = nullptr;
+      return (int)e;
+    }
+    capacity = m;
+    return 0;
+  }
+};
+
+} // namespace
+
+int sortEdgesToHost(DeviceEdges &edges, int m, cudaStream_t s, std::vector<int> &u,
+                    std::vector<int> &v, std::vector<float> &w) {
+  u.resize(m);
+  v.resize(m);
+  w.resize(m);
+  if (m == 0)
+    return 0;
+  StatusChain st;
+  DeviceBuffer<int> uo, vo;
+  DeviceBuffer<float> wo;
+  CUHC_TRY(st, uo.allocate(m, s));
+  CUHC_TRY(st, vo.allocate(m, s));
+  CUHC_TRY(st, wo.allocate(m, s));
+  CUHC_TRY(st, sortEdgesOnDevice(edges, m, s, uo, vo, wo));
   CUHC_TRY(st, cudaMemcpyAsync(u.data(), uo.get(), m * sizeof(int), cudaMemcpyDeviceToHost, s));
   CUHC_TRY(st, cudaMemcpyAsync(v.data(), vo.get(), m * sizeof(int), cudaMemcpyDeviceToHost, s));
   CUHC_TRY(st, cudaMemcpyAsync(w.data(), wo.get(), m * sizeof(float), cudaMemcpyDeviceToHost, s));
   CUHC_TRY(st, cudaStreamSynchronize(s));
+  return st.code;
+}
+
+int sortEdgesToPinned(DeviceEdges &edges, int m, cudaStream_t s, HostEdges &out) {
+  static thread_local PinnedEdgeBuffers pinned;
+  out = HostEdges{};
+  if (m == 0)
+    return 0;
+  StatusChain st;
+  CUHC_TRY(st, pinned.reserve((size_t)m));
+  if (!st.ok())
+    return st.code;
+  int *hu = static_cast<int *>(pinned.data);
+  int *hv = hu + pinned.capacity;
+  float *hw = reinterpret_cast<float *>(hv + pinned.capacity);
+  DeviceBuffer<int> uo, vo;
+  DeviceBuffer<float> wo;
+  CUHC_TRY(st, uo.allocate(m, s));
+  CUHC_TRY(st, vo.allocate(m, s));
+  CUHC_TRY(st, wo.allocate(m, s));
+  CUHC_TRY(st, sortEdgesOnDevice(edges, m, s, uo, vo, wo));
+  CUHC_TRY(st, cudaMemcpyAsync(hu, uo.get(), m * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUHC_TRY(st, cudaMemcpyAsync(hv, vo.get(), m * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUHC_TRY(st, cudaMemcpyAsync(hw, wo.get(), m * sizeof(float), cudaMemcpyDeviceToHost, s));
+  CUHC_TRY(st, cudaStreamSynchronize(s));
+  if (st.ok())
+    out = HostEdges{hu, hv, hw, m};
   return st.code;
 }
 
@@ -114,10 +180,14 @@ void treeFromOrderedMerges(const int *u, const int *v, const float *w, int n, do
     int parent, size, id, unused;
   };
   constexpr int kPrefetch = 16;
-  std::vector<Node> node(n);
+  // Reused by the thread's later calls: a fresh 16-byte record per point
+  // would cost a page fault per 256 points on every call.
+  static thread_local std::vector<Node> node;
+  if (node.size() < (size_t)n)
+    node.resize(n);
   for (int i = 0; i < n; ++i)
     node[i] = {i, 1, i, 0};
-  auto find = [&node](int x) {
+  auto find = [](int x) {
     while (node[x].parent != x) {
       node[x].parent = node[node[x].parent].parent;
       x = node[x].parent;
