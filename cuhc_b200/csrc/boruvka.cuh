@@ -30,6 +30,17 @@
 #include "screen.cuh"
 
 namespace cuhc {
+// Whether the index's data suits the metric's tensor-core screen (callers
+// check useScreen too): coordinate extents for every screened metric, and for
+// cosine the range of the points' squared norms.
+template <class Metric> inline bool screenDataOk(SpatialIndex &index) {
+  if (!index.extentsWithin(kScreenMaxExtent))
+    return false;
+  if constexpr (std::is_same<Metric, CosineMetric>::value)
+    return index.normsWithin(kCosineNormLow, kCosineNormHigh);
+  return true;
+}
+
 namespace boruvka_detail {
 
 inline int blocks(long long work, int threads = 256) { return (int)((work + threads - 1) / threads); }
@@ -270,7 +281,7 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
   p.screenAudit = screenAuditWords();
   p.rootOfTile = index.numInstances > 1 ? index.rootOfTile.get() : nullptr;
 
-  const bool screened = useScreen<Metric>(index.d, 0) && index.extentsWithin(kScreenMaxExtent);
+  const bool screened = useScreen<Metric>(index.d, 0) && screenDataOk<Metric>(index);
   DeviceBuffer<int> packed;
   if (screened)
     CUHC_TRY(st, packed.allocate((size_t)index.numTiles * 3 * kTile, stream));
@@ -379,9 +390,17 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
       else
         CUHC_TRY(rs, (launchPass<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
       if (useRadius) {
-        // Certify; the rest search again with no cap while certified rows sit out.
+        // Certify by component; the rest search again with no cap while
+        // certified rows sit out. compBest already holds real edge weights
+        // (seeds from the last round, and what rows published during the
+        // pass); every row's final best goes in too, so it ends at most the
+        // lightest edge found, which is what certification compares with.
+        radius_detail::componentMinFound<<<blocks(n), 256, 0, stream>>>(
+            nearest.get(), index.order.get(), comp.get(), n, compBest.get());
+        noteLaunch();
         radius_detail::certifyRows<<<blocks(n), 256, 0, stream>>>(
-            nearest.get(), index.order.get(), n, radius.get(), certified.get());
+            nearest.get(), index.order.get(), comp.get(), compBest.get(), n, radius.get(),
+            certified.get());
         noteLaunch();
         if (screened)
           CUHC_TRY(rs, (launchScreen<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
@@ -567,7 +586,7 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
   p.rootOfTile = index.numInstances > 1 ? index.rootOfTile.get() : nullptr;
   {
     const bool screened =
-        useScreen<Metric>(index.d, k) && index.extentsWithin(kScreenMaxExtent);
+        useScreen<Metric>(index.d, k) && screenDataOk<Metric>(index);
     PassTimer timer(screened ? kTimerScreenKnnPass : kTimerKnnPass, stream);
     if (screened)
       CUHC_TRY(st, (launchScreen<Metric, PlainWeight, true>(p, metric, PlainWeight{}, index.kc,
@@ -640,7 +659,7 @@ float timeKnnSample(SpatialIndex &index, const Metric &metric, int k, bool scree
 // Whether this index's passes can run screened (metric, width, shared
 // memory, data extent), ignoring the screen mode's "off".
 template <class Metric> bool screenable(SpatialIndex &index, int k) {
-  return useScreen<Metric>(index.d, k) && index.extentsWithin(kScreenMaxExtent);
+  return useScreen<Metric>(index.d, k) && screenDataOk<Metric>(index);
 }
 
 } // namespace cuhc

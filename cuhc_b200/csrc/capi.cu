@@ -276,38 +276,23 @@ int batchTrees(const float *devPoints, const std::vector<int> &sizes,
   weight.alpha = 1.0f;
   DeviceEdges edges;
   CUHC_TRY(st, (boruvkaMst<Metric, MutualReachWeight>(index, m, weight, true, edges, &stats, s)));
-  std::vector<int> u, v;
-  std::vector<float> w;
-  CUHC_TRY(st, sortEdgesToHost(edges, edges.count, s, u, v, w));
-  if (st.ok() && (long long)u.size() != offsets[count] - count)
+  // Edges sorted by (instance, w, u, v) on the device, in local ids: instance
+  // i's n_i - 1 edges at slots offsets[i] - i ...; then every instance's tree
+  // on the host threads.
+  HostEdges sorted;
+  std::vector<int> edgeCounts;
+  CUHC_TRY(st, sortBatchEdgesToPinned(edges, edges.count, offsets, s, sorted, edgeCounts));
+  if (st.ok() && (long long)sorted.count != offsets[count] - count)
     st(kErrorDisconnected);
+  for (int i = 0; st.ok() && i < count; ++i)
+    if (edgeCounts[i] != sizes[i] - 1)
+      st(kErrorDisconnected);
   if (st.ok()) {
-    // Edges in (w, u, v) order, partitioned stably by instance (instance i's
-    // n_i - 1 edges at slots offsets[i] - i ...), in local ids; then every
-    // instance's tree on the host threads.
-    const size_t edgesTotal = u.size();
-    std::vector<int> lu(edgesTotal), lv(edgesTotal);
-    std::vector<float> lw(edgesTotal);
-    std::vector<long long> fill(count);
-    for (int i = 0; i < count; ++i)
-      fill[i] = offsets[i] - i;
-    for (size_t e = 0; e < edgesTotal; ++e) {
-      const int i = (int)(std::upper_bound(offsets.begin(), offsets.end(), (long long)u[e]) -
-                          offsets.begin()) - 1;
-      const long long at = fill[i]++;
-      if (at >= offsets[i + 1] - (i + 1)) {
-        st(kErrorDisconnected); // more edges than the instance's tree has
-        break;
-      }
-      lu[at] = u[e] - (int)offsets[i];
-      lv[at] = v[e] - (int)offsets[i];
-      lw[at] = w[e];
-    }
     std::atomic<int> next{0};
     auto worker = [&]() {
       for (int i = next++; i < count; i = next++) {
         const long long first = offsets[i] - i;
-        treeFromOrderedMerges(lu.data() + first, lv.data() + first, lw.data() + first, sizes[i],
+        treeFromOrderedMerges(sorted.u + first, sorted.v + first, sorted.w + first, sizes[i],
                               hostTrees + first * 4);
       }
     };

@@ -14,7 +14,13 @@
 //                      filter(acc) <= filterBound(dist).
 // A pair whose filter value exceeds the bound of the row's current best can
 // not win, so the exact epilogue (sqrt, weight, key compare) runs only for
-// the few pairs that pass.
+// the few pairs that pass. Metrics with a tensor-core screen (screen.cuh)
+// also give
+//   screenBound(dist)  the bound on the screened value: the screen's value of
+//                      a pair is at most its exact value's image here, so a
+//                      pair with distance <= dist has screened value <=
+//                      screenBound(dist) (the squared distance for the
+//                      Euclidean metrics, the distance itself for cosine).
 //
 // Every built-in metric treats a zero-padded feature pair (0, 0) as an exact
 // no-op (fmaf(0,0,acc) == acc, acc + |0| == acc, fmax(acc, 0) == acc for
@@ -60,11 +66,13 @@ struct SqEuclideanMetric {
   CUHC_HD float finalize(Acc acc) const { return acc; }
   __device__ __forceinline__ float filter(Acc acc) const { return acc; }
   __device__ __forceinline__ float filterBound(float dist) const { return dist; }
+  __device__ __forceinline__ float screenBound(float dist) const { return dist; }
 };
 
 struct EuclideanMetric : SqEuclideanMetric {
   CUHC_HD float finalize(Acc acc) const { return sqrtf(acc); }
   __device__ __forceinline__ float filterBound(float dist) const { return sqBound(dist); }
+  __device__ __forceinline__ float screenBound(float dist) const { return sqBound(dist); }
 };
 
 struct ManhattanMetric {
@@ -141,6 +149,8 @@ struct CosineMetric {
   // No cheap monotone proxy: every pair takes the exact path.
   __device__ __forceinline__ float filter(Acc) const { return 0.0f; }
   __device__ __forceinline__ float filterBound(float) const { return INFINITY; }
+  // The screen bounds the distance itself.
+  __device__ __forceinline__ float screenBound(float dist) const { return dist; }
 };
 
 // Relative slack of the box lower bound: a pair's computed distance and the

@@ -38,6 +38,13 @@ struct HostEdges {
   int count = 0;
 };
 int sortEdgesToPinned(DeviceEdges &edges, int numEdges, cudaStream_t stream, HostEdges &out);
+// Edges of a batch (original ids = rows of the concatenated points, instance
+// i owning rows offsets[i] .. offsets[i + 1] - 1): sorted by (instance,
+// weight, u, v) on the device, endpoints in each instance's local ids, into
+// the same thread-owned page-locked buffers; counts[i] = instance i's edges.
+int sortBatchEdgesToPinned(DeviceEdges &edges, int numEdges,
+                           const std::vector<long long> &offsets, cudaStream_t stream,
+                           HostEdges &out, std::vector<int> &counts);
 
 // scipy linkage rows from merges in tree order (each merge after the merges
 // that made its clusters): union-find names clusters, as the reference's

@@ -6,12 +6,19 @@
 // in the previous round (0 in round 0). The MLP of mlp.cu predicts the log of
 // the row's nearest other-component weight; the proposed radius is
 // exp(prediction + offset), offset a calibration margin stored with the
-// model. The pass runs with every row's threshold capped by its radius. A row
-// whose best edge weighs at most its radius is certified: any lighter pair
-// would lie inside the radius and would have been found, so its result is
-// the exact one. Every other row (its lightest pair lies outside the radius)
-// is searched again in a fallback pass with no cap while certified rows sit
-// out. Results never depend on the model; a poor one only costs time.
+// model. The pass runs with every row's threshold capped by its radius.
+// Borůvka needs each component's lightest edge, not each row's, so rows are
+// certified per component: with m_C the lightest edge weight any row of
+// component C found, a row is done when its best edge weighs at most its
+// radius (any lighter pair would lie inside the radius and would have been
+// found) or when its radius is at least m_C (every pair of the row up to
+// m_C, ties included, was searched, and nothing heavier can be C's lightest
+// edge). m_C may also be lowered by any other real edge of C known (the
+// component best of the round: last round's edges that leave C). Only the
+// other rows -- a radius below m_C and nothing found inside it -- search
+// again, in a fallback pass with no cap, whose component bests start at m_C,
+// while certified rows sit out. Results never depend on the model; a poor one
+// only costs time.
 #pragma once
 
 #include <vector>
@@ -90,17 +97,35 @@ static __global__ void radiusFromPrediction(const float *__restrict__ prediction
     radius[pos] = order[pos] < 0 ? -1.0f : expf(prediction[pos] + offset);
 }
 
-// After the capped pass: certified rows get -1 (settled), the others +inf
-// (searched again, uncapped); counts the certified rows.
+// After the capped pass: lowers compMin[comp] (float bits of real edge
+// weights) to the lightest edge any row of the component found.
+static __global__ void componentMinFound(const unsigned long long *__restrict__ nearest,
+                                         const int *__restrict__ order,
+                                         const int *__restrict__ comp, int n,
+                                         unsigned int *__restrict__ compMin) {
+  const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pos >= n || order[pos] < 0)
+    return;
+  const unsigned long long key = nearest[pos];
+  if (key != kEmptyKey)
+    atomicMin(&compMin[comp[pos]], (unsigned int)(key >> 32));
+}
+
+// Certification by component (see the header): certified rows get -1
+// (settled, their capped result stands), the others +inf (searched again,
+// uncapped); counts the certified rows.
 static __global__ void certifyRows(const unsigned long long *__restrict__ nearest,
-                                   const int *__restrict__ order, int n,
+                                   const int *__restrict__ order, const int *__restrict__ comp,
+                                   const unsigned int *__restrict__ compMin, int n,
                                    float *__restrict__ radius,
                                    unsigned long long *__restrict__ certified) {
   const int pos = blockIdx.x * blockDim.x + threadIdx.x;
   if (pos >= n || order[pos] < 0)
     return;
   const unsigned long long key = nearest[pos];
-  const bool ok = key != kEmptyKey && keyWeight(key) <= radius[pos];
+  const float r = radius[pos];
+  const bool inside = key != kEmptyKey && keyWeight(key) <= r;
+  const bool ok = inside || r >= __uint_as_float(compMin[comp[pos]]);
   radius[pos] = ok ? -1.0f : INFINITY;
   if (ok)
     atomicAdd(certified, 1ull);

@@ -85,6 +85,31 @@ constexpr float kIndicator = 0x1p90f;
 constexpr float kScreenAbsSlack = 0x1p-70f;
 constexpr float kScreenMaxExtent = 0x1p40f;
 
+// Cosine. The screen runs on unit vectors: x^ = a rsqrt(|a|^2) (0 for a zero
+// point), y^ likewise, and one MMA gives D'(i, j) = c - sum_k tf32(x^_k)
+// tf32(y^_k) with c = 1 - e rounded down to TF32. e (screenMarginCosine) is
+// twice a bound of every error against the reference's FP32 distance
+// 1 - (a.b) / sqrt(|a|^2 |b|^2) (distances.cuh:69-83): the TF32 products, the
+// normalisation, the tensor core's accumulation (modelled as for the
+// Euclidean screen) and the reference's own rounding (dot product, norms,
+// square root, division, 1 - q), all relative to sum |x^_k y^_k| + 1 <= 2
+// (Cauchy-Schwarz). Hence D' <= the reference's distance for every pair,
+// provided no norm product underflows or overflows there (the reference then
+// returns 1 whatever the angle): the screen needs every nonzero point's
+// squared norm in [2^-60, 2^60] (SpatialIndex::normsWithin); other data runs
+// plain. A zero point screens at c < 1, its reference distance being 1.
+constexpr float kCosineNormLow = 0x1p-60f;
+constexpr float kCosineNormHigh = 0x1p60f;
+
+inline float screenMarginCosine(int d, int kc) {
+  const double u = std::ldexp(1.0, -24), t = std::ldexp(1.0, -11), u22 = std::ldexp(1.0, -22);
+  const double product = t * (2.0 + t);                 // tf32(x^) tf32(y^) against x^ y^
+  const double normalise = 8.0 * u;                     // rsqrtf (2 ulp) and the scaling
+  const double mma = 4.0 * screenKPad(kc) * u22 * 2.01; // accumulation, four times over
+  const double reference = (2.0 * d + 8.0) * u;         // the reference's FP32 chain
+  return (float)(2.0 * (product + normalise + mma + reference));
+}
+
 // e of the header comment, for d features staged as chunks of kc.
 inline float screenMargin(int d, int kc) {
   const double u = std::ldexp(1.0, -24), t = std::ldexp(1.0, -11), u22 = std::ldexp(1.0, -22);
@@ -256,6 +281,61 @@ __device__ __forceinline__ void buildColumnOperand(const float *raw, const int *
   storeOperandRow<kPad>(opB, j, val);
 }
 
+// Cosine operands: the reciprocal norm of a point (0 for a zero point), its
+// squared norm folded in feature order as the reference does.
+template <int KC>
+__device__ __forceinline__ float unitScale(const float *x, int stride, int i) {
+  float n = 0.0f;
+#pragma unroll
+  for (int k = 0; k < KC; ++k)
+    n = fmaf(x[k * stride + i], x[k * stride + i], n);
+  return n > 0.0f ? rsqrtf(n) : 0.0f;
+}
+
+// Row operand of row tile point i (cosine): [x^ (KC), 1, 0, 0, 0, indicators].
+template <int KC>
+__device__ __forceinline__ void buildRowOperandCosine(const float *sA, int i, bool valid, int comp,
+                                                      const ScreenSync &ss, float *opA) {
+  constexpr int kPad = screenKPad(KC), R = screenSlots(KC);
+  float val[kPad];
+  const float r = unitScale<KC>(sA, kTile, i);
+#pragma unroll
+  for (int k = 0; k < KC; ++k)
+    val[k] = toTf32(sA[k * kTile + i] * r);
+  val[KC] = 1.0f;
+  val[KC + 1] = 0.0f;
+  val[KC + 2] = 0.0f;
+  val[KC + 3] = 0.0f;
+#pragma unroll
+  for (int q = 0; q < R; ++q)
+    val[KC + 4 + q] =
+        (ss.oneHot && valid && q < ss.rowSetCount && comp == ss.rowSet[q]) ? kIndicator : 0.0f;
+  storeOperandRow<kPad>(opA, i, val);
+}
+
+// Column operand of staged point j (cosine): [-y^ (KC), c, 0, 0, 0,
+// indicators], c = 1 - e rounded down to TF32.
+template <int KC>
+__device__ __forceinline__ void buildColumnOperandCosine(const float *raw, const int *comp,
+                                                         float c, int j, bool oneHot,
+                                                         const ScreenSync &ss, float *opB) {
+  constexpr int kPad = screenKPad(KC), R = screenSlots(KC);
+  float val[kPad];
+  const float r = unitScale<KC>(raw, kTile, j);
+#pragma unroll
+  for (int k = 0; k < KC; ++k)
+    val[k] = -toTf32(raw[k * kTile + j] * r);
+  val[KC] = c;
+  val[KC + 1] = 0.0f;
+  val[KC + 2] = 0.0f;
+  val[KC + 3] = 0.0f;
+  const int cj = oneHot ? comp[j] : INT_MIN;
+#pragma unroll
+  for (int q = 0; q < R; ++q)
+    val[KC + 4 + q] = (oneHot && q < ss.rowSetCount && cj == ss.rowSet[q]) ? 1.0f : 0.0f;
+  storeOperandRow<kPad>(opB, j, val);
+}
+
 // Audit of one computed tile (cuhc_set_screen_audit; one consumer warp, its
 // accumulator still held): every valid pair of the warp's rows -- a real
 // column point, and in Borůvka passes another component -- has its screened
@@ -293,21 +373,41 @@ __device__ __noinline__ void auditTile(unsigned long long *words, uint32_t taddr
       if (!kKnn && (useComp ? cComp[jj] : cOrig[jj]) == myComp)
         continue;
       typename Metric::Acc acc = m.init();
-      double s64 = 0.0, nj = 0.0;
+      double s, s64, norms;
+      if constexpr (std::is_same<Metric, CosineMetric>::value) {
+        // The screened value bounds the distance itself; the margin is
+        // absolute (norms = 1).
+        double dot = 0.0, na = 0.0, nb = 0.0;
 #pragma unroll
-      for (int k = 0; k < KC; ++k) {
-        const float b = raw[k * kTile + jj];
-        acc = m.accumulate(acc, a[k], b);
-        const double diff = (double)a[k] - (double)b;
-        s64 = fma(diff, diff, s64);
-        const float y = b - centre[k];
-        nj = fma((double)y, (double)y, nj);
+        for (int k = 0; k < KC; ++k) {
+          const float b = raw[k * kTile + jj];
+          acc = m.accumulate(acc, a[k], b);
+          dot = fma((double)a[k], (double)b, dot);
+          na = fma((double)a[k], (double)a[k], na);
+          nb = fma((double)b, (double)b, nb);
+        }
+        s = (double)m.finalize(acc);
+        s64 = na * nb > 0.0 ? 1.0 - dot / sqrt(na * nb) : 1.0;
+        norms = 1.0;
+      } else {
+        double nj = 0.0;
+        s64 = 0.0;
+#pragma unroll
+        for (int k = 0; k < KC; ++k) {
+          const float b = raw[k * kTile + jj];
+          acc = m.accumulate(acc, a[k], b);
+          const double diff = (double)a[k] - (double)b;
+          s64 = fma(diff, diff, s64);
+          const float y = b - centre[k];
+          nj = fma((double)y, (double)y, nj);
+        }
+        s = (double)acc;
+        norms = ni + nj;
       }
-      const double s = (double)acc, dp = (double)v[c];
+      const double dp = (double)v[c];
       ++pairs;
       if (dp > s + 0x1p-70)
         ++violations;
-      const double norms = ni + nj;
       // The relative margin is the guarantee where it exceeds the absolute
       // 2^-70 (below it, flushed and underflowed products are covered by
       // the absolute term alone, and D' <= s + 2^-70 is what counts).
@@ -382,6 +482,10 @@ __global__ void __launch_bounds__(kThreads, 2)
   const bool useComp = !kKnn && p.component != nullptr;
   const bool useValue = !kKnn && w.value != nullptr;
   const float scale = 1.0f - margin;
+  constexpr bool kCos = std::is_same<Metric, CosineMetric>::value;
+  // Cosine: 1 - e rounded down to TF32 (10 mantissa bits; the FP32 rounding of
+  // 1 - e is far inside the margin's factor two).
+  const float cosC = __uint_as_float(__float_as_uint(1.0f - margin) & ~0x1fffu);
 
   // Consumer row state (thread = row).
   const int myRow = tid & (kTile - 1);
@@ -472,7 +576,10 @@ __global__ void __launch_bounds__(kThreads, 2)
   const uint32_t tmem = ss.tmemBase;
   const bool oneHot = ss.oneHot != 0;
   if (consumer) {
-    buildRowOperand<KC>(sA, centre, scale, myRow, mySearch, myComp, ss, opA);
+    if constexpr (kCos)
+      buildRowOperandCosine<KC>(sA, myRow, mySearch, myComp, ss, opA);
+    else
+      buildRowOperand<KC>(sA, centre, scale, myRow, mySearch, myComp, ss, opA);
 #pragma unroll
     for (int k = 0; k < KC; ++k) {
       float lo = mySearch ? sA[k * kTile + myRow] : INFINITY;
@@ -499,7 +606,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     float thr;
     if (kKnn) {
       thr = listKeyValue(lists[myRow * p.k + p.k - 1]);
-      F = mySearch ? m.filterBound(thr) : -INFINITY;
+      F = mySearch ? m.screenBound(thr) : -INFINITY;
     } else {
       thr = rowBest == kEmptyKey ? INFINITY : keyWeight(rowBest);
       if (compSlot) {
@@ -512,7 +619,7 @@ __global__ void __launch_bounds__(kThreads, 2)
       if (mySearch && p.radius)
         thr = fminf(thr, p.radius[myPos]);
       F = (mySearch && thr >= 0.0f && w.feasible(thr, myVal))
-              ? m.filterBound(w.distBound(thr, myVal))
+              ? m.screenBound(w.distBound(thr, myVal))
               : -INFINITY;
     }
     return F == -INFINITY ? -INFINITY : thr;
@@ -771,7 +878,10 @@ __global__ void __launch_bounds__(kThreads, 2)
           float *b = opB + (size_t)s * kTile * kPad;
 #pragma unroll
           for (int q = j; q < kTile; q += kBuilderThreads)
-            buildColumnOperand<KC>(raw, comp, centre, scale, q, oneHot, ss, b);
+            if constexpr (kCos)
+              buildColumnOperandCosine<KC>(raw, comp, cosC, q, oneHot, ss, b);
+            else
+              buildColumnOperand<KC>(raw, comp, centre, scale, q, oneHot, ss, b);
         }
         fenceProxyAsync();
         __syncwarp();
@@ -904,7 +1014,7 @@ __global__ void __launch_bounds__(kThreads, 2)
                   const float old = rowKth;
                   rowKth = listKeyValue(list[p.k - 1]);
                   tie = (old < INFINITY && rowKth == old) ? 1 : 0;
-                  Fs = m.filterBound(rowKth) + kScreenAbsSlack;
+                  Fs = m.screenBound(rowKth) + kScreenAbsSlack;
                   dirty = true;
                 } else if (value == rowKth) {
                   tie = 1;
@@ -1038,6 +1148,9 @@ template <> struct ScreenSupport<EuclideanMetric> {
 template <> struct ScreenSupport<SqEuclideanMetric> {
   static constexpr bool value = true;
 };
+template <> struct ScreenSupport<CosineMetric> {
+  static constexpr bool value = true;
+};
 
 // Shared memory a block may use on sm_100 (227 KiB), and what each of two
 // blocks on one SM may use (228 KiB per SM, 1 KiB of it reserved per block).
@@ -1099,7 +1212,9 @@ int launchScreen(const PassParams &p, const Metric &m, const Weight &w, int kc,
   } else {
     if (p.numChunks != 1 || kc != chunkWidthFor(p.d))
       return kErrorInvalidAlgorithm;
-    const float margin = screenMargin(p.d, kc);
+    const float margin = std::is_same<Metric, CosineMetric>::value
+                             ? screenMarginCosine(p.d, kc)
+                             : screenMargin(p.d, kc);
     const int stages = screenStagesFor(p.d, kKnn ? p.k : 0);
     if (stages == 0)
       return kErrorInvalidAlgorithm;

@@ -3,6 +3,7 @@
 #include "spatial.cuh"
 
 #include <algorithm>
+#include <cstring>
 #include <vector>
 #include <cub/device/device_radix_sort.cuh>
 
@@ -474,6 +475,7 @@ int SpatialIndex::buildCommon(const float *points, int positions, int d_, bool s
 }
 
 int SpatialIndex::retile(const float *pointsByPosition, int newN) {
+  normRangeKnown = false;
   StatusChain st;
   n = newN;
   if (pointsByPosition) {
@@ -536,6 +538,54 @@ bool SpatialIndex::extentsWithin(float limit) {
     if (!(high[f] - low[f] <= limit)) // NaN fails too
       return false;
   return true;
+}
+
+namespace {
+
+// out[0] <- smallest nonzero squared norm, out[1] <- largest (float bits;
+// squared norms are >= 0, so their bits order like the values), over the
+// points of the tiled layout (padding slots skipped).
+__global__ void normRange(const float *__restrict__ tiled, const int *__restrict__ order, int n,
+                          int d, int kc, size_t tileFloats, unsigned int *__restrict__ out) {
+  const int pos = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pos >= n || order[pos] < 0)
+    return;
+  const float *tile = tiled + (size_t)(pos / kTile) * tileFloats;
+  float sq = 0.0f;
+  for (int k = 0; k < d; ++k) {
+    const float x = tile[(size_t)((k / kc) * kc + k % kc) * kTile + pos % kTile];
+    sq = fmaf(x, x, sq);
+  }
+  const unsigned int bits = __float_as_uint(sq);
+  if (sq > 0.0f)
+    atomicMin(out, bits);
+  atomicMax(out + 1, bits);
+}
+
+} // namespace
+
+bool SpatialIndex::normsWithin(float low, float high) {
+  if (normRangeKnown)
+    return normLow >= low && normHigh <= high;
+  DeviceBuffer<unsigned int> range;
+  unsigned int host[2] = {0x7f800000u, 0u};
+  if (range.allocate(2, stream) != 0 ||
+      cudaMemcpyAsync(range.get(), host, sizeof(host), cudaMemcpyHostToDevice, stream) !=
+          cudaSuccess)
+    return false;
+  normRange<<<(n + 255) / 256, 256, 0, stream>>>(tiled.get(), order.get(), n, d, kc,
+                                                 tileFloats(), range.get());
+  noteLaunch();
+  if (cudaGetLastError() != cudaSuccess ||
+      cudaMemcpyAsync(host, range.get(), sizeof(host), cudaMemcpyDeviceToHost, stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess)
+    return false;
+  std::memcpy(&normLow, &host[0], sizeof(float));
+  std::memcpy(&normHigh, &host[1], sizeof(float));
+  normRangeKnown = true;
+  // No nonzero point: the low end is +inf, which passes any bound.
+  return normLow >= low && normHigh <= high;
 }
 
 namespace {

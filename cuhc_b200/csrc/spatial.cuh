@@ -91,6 +91,11 @@ struct SpatialIndex {
   // finite and at most `limit`. Copies the root box to the host and waits
   // for the index stream.
   bool extentsWithin(float limit);
+  // Whether every point's squared norm is 0 or within [low, high] (the
+  // cosine screen's range). Computed once per index; retile resets it.
+  bool normsWithin(float low, float high);
+  bool normRangeKnown = false;
+  float normLow = 0.0f, normHigh = 0.0f;
   // tileOrder <- row tiles by decreasing tileWork (fromBoxes: by decreasing
   // leaf box log-volume, the estimate before any pass has run). Enqueued on
   // the index stream with no host work (buffers are allocated on first use).

@@ -129,8 +129,108 @@ int sortEdgesToHost(DeviceEdges &edges, int m, cudaStream_t s, std::vector<int> 
   return st.code;
 }
 
-int sortEdgesToPinned(DeviceEdges &edges, int m, cudaStream_t s, HostEdges &out) {
+namespace {
+
+// Instance of each sorted edge (the last i with offsets[i] <= u) and its
+// endpoints in the instance's local ids; counts[i] += 1.
+__global__ void localiseEdges(const long long *__restrict__ offsets, int count,
+                              int *__restrict__ u, int *__restrict__ v,
+                              int *__restrict__ instance, int *__restrict__ counts, int m) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m)
+    return;
+  int lo = 0, hi = count; // offsets[lo] <= u[e] < offsets[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) / 2;
+    if (offsets[mid] <= u[e])
+      lo = mid;
+    else
+      hi = mid;
+  }
+  instance[e] = lo;
+  u[e] -= (int)offsets[lo];
+  v[e] -= (int)offsets[lo];
+  atomicAdd(&counts[lo], 1);
+}
+
+PinnedEdgeBuffers &threadPinnedEdges() {
   static thread_local PinnedEdgeBuffers pinned;
+  return pinned;
+}
+
+} // namespace
+
+int sortBatchEdgesToPinned(DeviceEdges &edges, int m, const std::vector<long long> &offsets,
+                           cudaStream_t s, HostEdges &out, std::vector<int> &counts) {
+  out = HostEdges{};
+  const int count = (int)offsets.size() - 1;
+  counts.assign(count, 0);
+  if (m == 0)
+    return 0;
+  PinnedEdgeBuffers &pinned = threadPinnedEdges();
+  StatusChain st;
+  CUHC_TRY(st, pinned.reserve((size_t)m));
+  if (!st.ok())
+    return st.code;
+  int *hu = static_cast<int *>(pinned.data);
+  int *hv = hu + pinned.capacity;
+  float *hw = reinterpret_cast<float *>(hv + pinned.capacity);
+  DeviceBuffer<int> uo, vo, instance, instanceOut, perm, permOut, ug, vg, devCounts;
+  DeviceBuffer<float> wo, wg;
+  DeviceBuffer<long long> devOffsets;
+  CUHC_TRY(st, uo.allocate(m, s));
+  CUHC_TRY(st, vo.allocate(m, s));
+  CUHC_TRY(st, wo.allocate(m, s));
+  CUHC_TRY(st, instance.allocate(m, s));
+  CUHC_TRY(st, instanceOut.allocate(m, s));
+  CUHC_TRY(st, perm.allocate(m, s));
+  CUHC_TRY(st, permOut.allocate(m, s));
+  CUHC_TRY(st, ug.allocate(m, s));
+  CUHC_TRY(st, vg.allocate(m, s));
+  CUHC_TRY(st, wg.allocate(m, s));
+  CUHC_TRY(st, devCounts.allocate(count, s));
+  CUHC_TRY(st, devOffsets.allocate(count + 1, s));
+  if (!st.ok())
+    return st.code;
+  CUHC_TRY(st, cudaMemcpyAsync(devOffsets.get(), offsets.data(), (count + 1) * sizeof(long long),
+                               cudaMemcpyHostToDevice, s));
+  CUHC_TRY(st, cudaMemsetAsync(devCounts.get(), 0, count * sizeof(int), s));
+  CUHC_TRY(st, sortEdgesOnDevice(edges, m, s, uo, vo, wo));
+  const int blocks = (m + 255) / 256;
+  localiseEdges<<<blocks, 256, 0, s>>>(devOffsets.get(), count, uo.get(), vo.get(),
+                                       instance.get(), devCounts.get(), m);
+  noteLaunch();
+  iota<<<blocks, 256, 0, s>>>(perm.get(), m); noteLaunch();
+  // Stable by instance: each instance's edges keep their (w, u, v) order.
+  int bits = 1;
+  while ((1 << bits) < count)
+    ++bits;
+  size_t tempBytes = 0;
+  CUHC_TRY(st, cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, instance.get(),
+                                               instanceOut.get(), perm.get(), permOut.get(), m,
+                                               0, bits, s));
+  DeviceBuffer<unsigned char> temp;
+  CUHC_TRY(st, temp.allocate(std::max<size_t>(tempBytes, 1), s));
+  CUHC_TRY(st, cub::DeviceRadixSort::SortPairs(temp.get(), tempBytes, instance.get(),
+                                               instanceOut.get(), perm.get(), permOut.get(), m,
+                                               0, bits, s));
+  gatherEdges<<<blocks, 256, 0, s>>>(permOut.get(), uo.get(), vo.get(), wo.get(), ug.get(),
+                                     vg.get(), wg.get(), m);
+  noteLaunch();
+  CUHC_TRY(st, cudaGetLastError());
+  CUHC_TRY(st, cudaMemcpyAsync(hu, ug.get(), m * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUHC_TRY(st, cudaMemcpyAsync(hv, vg.get(), m * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUHC_TRY(st, cudaMemcpyAsync(hw, wg.get(), m * sizeof(float), cudaMemcpyDeviceToHost, s));
+  CUHC_TRY(st, cudaMemcpyAsync(counts.data(), devCounts.get(), count * sizeof(int),
+                               cudaMemcpyDeviceToHost, s));
+  CUHC_TRY(st, cudaStreamSynchronize(s));
+  if (st.ok())
+    out = HostEdges{hu, hv, hw, m};
+  return st.code;
+}
+
+int sortEdgesToPinned(DeviceEdges &edges, int m, cudaStream_t s, HostEdges &out) {
+  PinnedEdgeBuffers &pinned = threadPinnedEdges();
   out = HostEdges{};
   if (m == 0)
     return 0;

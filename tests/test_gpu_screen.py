@@ -99,3 +99,62 @@ def test_large_screen_matches_plain(modes):
     Y = normal(100000, 32, seed=4)
     np.testing.assert_array_equal(modes("on", "auto", lambda: C.linkage(Y, "single")),
                                   modes("off", "auto", lambda: C.linkage(Y, "single")))
+
+
+def cosine_cases():
+    """Cosine data: blobs, the same with every point scaled by a random
+    factor in [1e-6, 1e6] (the distance ignores it; squared norms stay inside
+    the screen's [2^-60, 2^60]), zero points, exact duplicates and
+    antiparallel copies."""
+    rng = np.random.default_rng(21)
+    X = blobs(1500, 16, noise=0.1, seed=21)
+    scaled = (X * np.exp(rng.uniform(np.log(1e-6), np.log(1e6), (len(X), 1)))).astype(np.float32)
+    special = X[:400].copy()
+    special[:10] = 0.0                      # zero points: distance 1 to everything
+    special[10:60] = special[60:110]        # duplicates: distance 0
+    special[110:160] = -special[160:210]    # antiparallel: distance 2
+    return {"blobs": X, "scaled": scaled, "special": special}
+
+
+@pytest.mark.parametrize("case", ["blobs", "scaled", "special"])
+def test_cosine_screened(modes, case):
+    X = cosine_cases()[case]
+    ref = O.single_linkage(X, metric="cosine")
+    _lib.set_timing(True)
+    _lib.kernel_timing()
+    try:
+        Z = modes("on", "auto", lambda: C.linkage(X, "single", metric="cosine"))
+        timing = _lib.kernel_timing()
+    finally:
+        _lib.set_timing(False)
+    np.testing.assert_array_equal(Z, ref)
+    assert timing["screen_pass"][1] > 0, timing  # the screened kernel ran
+    Z_ref, core_ref = O.hdbscan_tree(X, 7, metric="cosine")
+    Z, core = modes("on", "auto", lambda: hdbscan_tree(X, 7, metric="cosine"))
+    np.testing.assert_array_equal(core, core_ref)
+    np.testing.assert_array_equal(Z, Z_ref)
+
+
+@pytest.mark.parametrize("d", [3, 8, 31, 32])
+def test_cosine_dimensions(modes, d):
+    X = normal(1200, d, seed=d)
+    ref = O.single_linkage(X, metric="cosine")
+    np.testing.assert_array_equal(
+        modes("on", "auto", lambda: C.linkage(X, "single", metric="cosine")), ref)
+
+
+def test_cosine_outside_norm_range_runs_plain(modes):
+    """Squared norms below 2^-60 (the reference's norm product could
+    underflow there): the screen steps aside and the plain pass gives the
+    oracle's tree."""
+    X = (normal(600, 6, seed=4) * np.float32(1e-20)).astype(np.float32)
+    ref = O.single_linkage(X, metric="cosine")
+    _lib.set_timing(True)
+    _lib.kernel_timing()
+    try:
+        Z = modes("on", "auto", lambda: C.linkage(X, "single", metric="cosine"))
+        timing = _lib.kernel_timing()
+    finally:
+        _lib.set_timing(False)
+    np.testing.assert_array_equal(Z, ref)
+    assert timing["screen_pass"][1] == 0, timing

@@ -148,3 +148,24 @@ def test_audit_reports_fp64_errors(audited):
     assert 0.0 <= audit["max_exact_rel"] < 16 * 2.0 ** -24 * 8, audit
     assert audit["max_bound_gap_rel_norms"] < 0.05, audit
     assert audit["min_slack"] > 0.25, audit
+
+
+@pytest.mark.parametrize("d", [3, 16, 32])
+def test_cosine_bound(audited, d):
+    """Cosine: the screened value bounds the reference's FP32 distance
+    1 - a.b / sqrt(|a|^2 |b|^2) (src/distances.cuh:69-83) for every pair, on
+    points scaled over twelve orders of magnitude, with zero points,
+    duplicates and antiparallel pairs (distances 1, 0 and 2)."""
+    rng = np.random.default_rng(d)
+    X = blobs(1200, d, noise=0.1, seed=d)
+    X = (X * np.exp(rng.uniform(np.log(1e-6), np.log(1e6), (len(X), 1)))).astype(np.float32)
+    X[:5] = 0.0
+    X[5:40] = X[40:75]
+    X[75:110] = -X[110:145]
+    Z = C.linkage(X, "single", metric="cosine")
+    Zh, core = hdbscan_tree(X, 5, metric="cosine")
+    assert_bound_held(min_pairs=len(X))
+    np.testing.assert_array_equal(Z, O.single_linkage(X, metric="cosine"))
+    Z_ref, core_ref = O.hdbscan_tree(X, 5, metric="cosine")
+    np.testing.assert_array_equal(core, core_ref)
+    np.testing.assert_array_equal(Zh, Z_ref)
