@@ -573,6 +573,9 @@ def run_tree_workload(args, local_rank):
             if radius:
                 results[name]["certified_share"] = round(
                     stats["certified"] / max(1, stats["proposed"]), 4)
+                results[name]["tiles_per_tree"] = {
+                    "capped_passes": stats["capped_tiles"] // max(1, args.steps),
+                    "fallback_passes": stats["fallback_tiles"] // max(1, args.steps)}
                 results[name]["model"] = (f"trained on seeds {list(meta['seeds'])}, n = "
                                           f"{int(meta['n'])}, {int(meta['rows'])} rows")
                 C.set_radius_model(None)

@@ -114,10 +114,13 @@ def load_radius_model(path=MODEL_PATH):
 
 
 def radius_stats():
-    """{'proposed': rows given a radius, 'certified': rows settled by it} since the last call."""
-    out = (ctypes.c_uint64 * 2)()
-    _lib.check(_L.cuhc_radius_stats(out, 2))
-    return {"proposed": int(out[0]), "certified": int(out[1])}
+    """Since the last call: rows given a radius ('proposed'), rows settled by
+    the capped pass ('certified'), tiles computed by the capped passes
+    ('capped_tiles') and by the fallback passes ('fallback_tiles')."""
+    out = (ctypes.c_uint64 * 4)()
+    _lib.check(_L.cuhc_radius_stats(out, 4))
+    return {"proposed": int(out[0]), "certified": int(out[1]), "capped_tiles": int(out[2]),
+            "fallback_tiles": int(out[3])}
 
 
 def init_params(seed=0):

@@ -319,8 +319,8 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
     CUHC_TRY(st, prediction.allocate(n, stream));
     CUHC_TRY(st, radius.allocate(n, stream));
     CUHC_TRY(st, targets.allocate(n, stream));
-    CUHC_TRY(st, certified.allocate(1, stream));
-    CUHC_TRY(st, cudaMemsetAsync(certified.get(), 0, sizeof(unsigned long long), stream));
+    CUHC_TRY(st, certified.allocate(4, stream)); // certified rows, then [mark, capped, fallback]
+    CUHC_TRY(st, cudaMemsetAsync(certified.get(), 0, 4 * sizeof(unsigned long long), stream));
   }
   auto enqueueFeatures = [&](int round) {
     StatusChain fs;
@@ -382,6 +382,8 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
       noteLaunch();
       p.radius = radius.get();
       proposedRows += (unsigned long long)index.numPoints;
+      radius_detail::radiusTileStep<<<1, 1, 0, stream>>>(tiles.get(), 0, certified.get() + 1);
+      noteLaunch();
     }
     {
       PassTimer timer(timed ? (screened ? kTimerScreenPass : kTimerNearestPass) : -1, stream);
@@ -395,6 +397,8 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
         // (seeds from the last round, and what rows published during the
         // pass); every row's final best goes in too, so it ends at most the
         // lightest edge found, which is what certification compares with.
+        radius_detail::radiusTileStep<<<1, 1, 0, stream>>>(tiles.get(), 1, certified.get() + 1);
+        noteLaunch();
         radius_detail::componentMinFound<<<blocks(n), 256, 0, stream>>>(
             nearest.get(), index.order.get(), comp.get(), n, compBest.get());
         noteLaunch();
@@ -406,6 +410,8 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
           CUHC_TRY(rs, (launchScreen<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
         else
           CUHC_TRY(rs, (launchPass<Metric, Weight, false>(p, metric, weight, index.kc, stream)));
+        radius_detail::radiusTileStep<<<1, 1, 0, stream>>>(tiles.get(), 2, certified.get() + 1);
+        noteLaunch();
         p.radius = nullptr;
       }
       if (timer.start) {
@@ -513,11 +519,10 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
     }
   }
   if (useRadius) {
-    unsigned long long certifiedRows = 0;
-    cudaMemcpyAsync(&certifiedRows, certified.get(), sizeof(certifiedRows), cudaMemcpyDeviceToHost,
-                    stream);
+    unsigned long long counts[4] = {};
+    cudaMemcpyAsync(counts, certified.get(), sizeof(counts), cudaMemcpyDeviceToHost, stream);
     cudaStreamSynchronize(stream);
-    addRadiusStats(proposedRows, certifiedRows);
+    addRadiusStats(proposedRows, counts[0], counts[2], counts[3]);
   }
   if (graphExec)
     cudaGraphExecDestroy(graphExec);

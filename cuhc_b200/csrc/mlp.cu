@@ -216,7 +216,8 @@ unsigned long long gModelVersion = 0;
 constexpr int kMaxDevices = 64;
 float *gModelDevice[kMaxDevices] = {};
 unsigned long long gModelDeviceVersion[kMaxDevices] = {};
-std::atomic<unsigned long long> gRadiusProposed{0}, gRadiusCertified{0};
+std::atomic<unsigned long long> gRadiusProposed{0}, gRadiusCertified{0}, gRadiusCappedTiles{0},
+    gRadiusFallbackTiles{0};
 } // namespace
 
 RadiusModel currentRadiusModel() {
@@ -243,9 +244,12 @@ RadiusModel currentRadiusModel() {
   return model;
 }
 
-void addRadiusStats(unsigned long long proposed, unsigned long long certified) {
+void addRadiusStats(unsigned long long proposed, unsigned long long certified,
+                    unsigned long long cappedTiles, unsigned long long fallbackTiles) {
   gRadiusProposed += proposed;
   gRadiusCertified += certified;
+  gRadiusCappedTiles += cappedTiles;
+  gRadiusFallbackTiles += fallbackTiles;
 }
 
 } // namespace cuhc
@@ -267,11 +271,14 @@ int cuhc_set_radius_model(const float *params, float offset) {
   return 0;
 }
 
-// Rows given a proposed radius, and rows the capped pass certified, since the
-// last call (first `count` of the two); resets them.
+// Since the last call (first `count` of the four; resets them): rows given a
+// proposed radius, rows the capped pass certified, tiles the capped passes
+// computed, tiles the fallback passes computed.
 int cuhc_radius_stats(unsigned long long *out, int count) {
-  const unsigned long long v[2] = {gRadiusProposed.exchange(0), gRadiusCertified.exchange(0)};
-  for (int i = 0; i < count && i < 2; ++i)
+  const unsigned long long v[4] = {gRadiusProposed.exchange(0), gRadiusCertified.exchange(0),
+                                   gRadiusCappedTiles.exchange(0),
+                                   gRadiusFallbackTiles.exchange(0)};
+  for (int i = 0; i < count && i < 4; ++i)
     out[i] = v[i];
   return 0;
 }

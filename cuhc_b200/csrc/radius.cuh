@@ -41,7 +41,8 @@ struct RadiusModel {
 };
 RadiusModel currentRadiusModel();
 // Counters: rows proposed, rows certified by the first pass.
-void addRadiusStats(unsigned long long proposed, unsigned long long certified);
+void addRadiusStats(unsigned long long proposed, unsigned long long certified,
+                    unsigned long long cappedTiles, unsigned long long fallbackTiles);
 
 // Logging of (features, target) rows for training, filled by a Borůvka run.
 struct RadiusLog {
@@ -95,6 +96,17 @@ static __global__ void radiusFromPrediction(const float *__restrict__ prediction
   const int pos = blockIdx.x * blockDim.x + threadIdx.x;
   if (pos < n)
     radius[pos] = order[pos] < 0 ? -1.0f : expf(prediction[pos] + offset);
+}
+
+// Tile accounting of the proposal's passes: acc = [mark, capped, fallback];
+// step 0 marks the pass counter, step 1 adds the tiles since the mark to the
+// capped tiles (and marks again), step 2 to the fallback tiles.
+static __global__ void radiusTileStep(const unsigned long long *__restrict__ tiles, int step,
+                                      unsigned long long *__restrict__ acc) {
+  const unsigned long long now = *tiles;
+  if (step > 0)
+    acc[step] += now - acc[0];
+  acc[0] = now;
 }
 
 // After the capped pass: lowers compMin[comp] (float bits of real edge

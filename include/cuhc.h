@@ -143,7 +143,8 @@ int cuhc_trees_batched_device(const float *devicePoints, const long long *offset
 /* Loads the model (HOST params) with its calibration offset (radius =
  * exp(prediction + offset)); params NULL switches the proposal off. */
 int cuhc_set_radius_model(const float *params, float offset);
-/* Rows proposed and rows certified since the last call (first `count`). */
+/* Since the last call (first `count` of: rows proposed, rows certified,
+ * tiles of the capped passes, tiles of the fallback passes). */
 int cuhc_radius_stats(unsigned long long *out, int count);
 /* Up to maxRowsPerRound random rows per exact single-linkage round of points
  * (HOST, n x 16): features [rows][19], targets (log nearest other-component
