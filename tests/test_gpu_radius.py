@@ -116,7 +116,7 @@ def test_shipped_model_gain_and_cost(no_model):
         _lib.set_timing(False)
         C.set_radius_model(None)
     np.testing.assert_array_equal(Z_model, Z_plain)
-    assert stats["certified"] > 0.8 * stats["proposed"], stats
+    assert stats["certified"] > 0.5 * stats["proposed"], stats
     assert 0 < stats["capped_tiles"] < tiles_without, (stats, tiles_without)
     assert stats["fallback_tiles"] > 0, stats
     print(f"tiles without the model {tiles_without:,}; with it: capped passes "
