@@ -472,7 +472,9 @@ def run_hdbscan(args, rank, world, local_rank):
             "config": workload_config("hdbscan", n, d),
             "setup": {"path": "tcgen05 TF32 screen + exact FP32 recheck",
                       "l2": "flushed before every step (256 MB write)",
-                      "parallelism": f"replicas x{world}"},
+                      "parallelism": f"replicas x{world}",
+                      "knn_pipeline_shape": dict(zip(("stages", "lead"), _lib.screen_shape()),
+                                                 chosen_by="shape tuner, first call")},
             "e2e": {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": int(X.nbytes),
                     "d2h_bytes_per_step": int((n - 1) * 4 * 8 + n * 4)},
             "gpu_launches": int(launches),

@@ -71,6 +71,8 @@ lib.cuhc_set_screen_audit.restype = _int
 lib.cuhc_set_screen_audit.argtypes = [_int]
 lib.cuhc_screen_audit.restype = _int
 lib.cuhc_screen_audit.argtypes = [_f64, _int]
+lib.cuhc_screen_shape.restype = _int
+lib.cuhc_screen_shape.argtypes = [ctypes.POINTER(_int), ctypes.POINTER(_int)]
 lib.cuhc_wait_selftest.restype = _int
 lib.cuhc_wait_selftest.argtypes = [_int, _int, _int]
 
@@ -182,3 +184,11 @@ def screen_audit():
     values = [float(x) for x in out]
     values[0], values[1] = int(values[0]), int(values[1])
     return dict(zip(AUDIT_FIELDS, values))
+
+
+def screen_shape():
+    """(ring slots, copy lead) the shape tuner chose for the latest screened
+    k-NN pass ((0, 0) before any)."""
+    stages, lead = _int(), _int()
+    check(lib.cuhc_screen_shape(ctypes.byref(stages), ctypes.byref(lead)))
+    return stages.value, lead.value

@@ -21,6 +21,10 @@
 #pragma once
 
 #include <algorithm>
+#include <typeinfo>
+#include <tuple>
+#include <mutex>
+#include <map>
 #include <random>
 #include <type_traits>
 
@@ -30,6 +34,20 @@
 #include "screen.cuh"
 
 namespace cuhc {
+// Sets the calling thread's screened pipeline shape for a scope.
+struct ScreenShapeScope {
+  ScreenShape previous;
+  explicit ScreenShapeScope(ScreenShape shape) : previous(currentScreenShape()) {
+    setScreenShape(shape);
+  }
+  ~ScreenShapeScope() { setScreenShape(previous); }
+};
+
+// Pipeline-shape tuner of the screened k-NN pass (defined below).
+template <class Metric>
+ScreenShape tunedScreenShape(SpatialIndex &index, const Metric &m, int k, float *scratch,
+                             cudaStream_t s);
+
 // Whether the index's data suits the metric's tensor-core screen (callers
 // check useScreen too): coordinate extents for every screened metric, and for
 // cosine the range of the points' squared norms.
@@ -592,6 +610,9 @@ int coreDistances(SpatialIndex &index, const Metric &metric, int k, bool prune, 
   {
     const bool screened =
         useScreen<Metric>(index.d, k) && screenDataOk<Metric>(index);
+    const ScreenShape shape =
+        screened ? tunedScreenShape<Metric>(index, metric, k, core, stream) : ScreenShape{};
+    ScreenShapeScope shapeScope(shape);
     PassTimer timer(screened ? kTimerScreenKnnPass : kTimerKnnPass, stream);
     if (screened)
       CUHC_TRY(st, (launchScreen<Metric, PlainWeight, true>(p, metric, PlainWeight{}, index.kc,
@@ -665,6 +686,51 @@ float timeKnnSample(SpatialIndex &index, const Metric &metric, int k, bool scree
 // memory, data extent), ignoring the screen mode's "off".
 template <class Metric> bool screenable(SpatialIndex &index, int k) {
   return useScreen<Metric>(index.d, k) && screenDataOk<Metric>(index);
+}
+
+// Pipeline-shape tuner of the screened k-NN pass: times candidate (ring
+// slots, copy lead) pairs -- the most slots that fit with leads 2-6, and the
+// fewest slots with lead 3 -- on the first 2 x SMs row tiles of the index
+// (twice each, the faster kept) and returns the fastest, cached per process
+// by (metric, d, k, batched or not). A shape changes time only, never a
+// result. `scratch` receives throw-away core distances (n floats).
+template <class Metric>
+ScreenShape tunedScreenShape(SpatialIndex &index, const Metric &m, int k, float *scratch,
+                             cudaStream_t s) {
+  static std::mutex mutex;
+  static std::map<std::tuple<size_t, int, int, bool>, ScreenShape> tuned;
+  const auto key = std::make_tuple(typeid(Metric).hash_code(), index.d, k, index.numInstances > 1);
+  {
+    std::lock_guard<std::mutex> lock(mutex);
+    const auto it = tuned.find(key);
+    if (it != tuned.end())
+      return it->second;
+  }
+  const int maxStages = screenStagesFor(index.d, k);
+  std::vector<ScreenShape> candidates;
+  for (int lead = 2; lead <= 6; ++lead)
+    if (lead <= maxStages - 1)
+      candidates.push_back(ScreenShape{maxStages, lead});
+  if (maxStages > kScreenMinStages)
+    candidates.push_back(ScreenShape{kScreenMinStages, 3});
+  int device = 0, sms = 148;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  ScreenShape best{};
+  float bestMs = INFINITY;
+  for (const ScreenShape shape : candidates) {
+    ScreenShapeScope scope(shape);
+    float ms = INFINITY;
+    for (int rep = 0; rep < 2; ++rep)
+      ms = std::min(ms, timeKnnSample(index, m, k, true, 2 * sms, scratch, s));
+    if (ms < bestMs) {
+      bestMs = ms;
+      best = shape;
+    }
+  }
+  std::lock_guard<std::mutex> lock(mutex);
+  tuned[key] = best;
+  return best;
 }
 
 } // namespace cuhc

@@ -23,6 +23,7 @@
 #include "metrics.cuh"
 #include "pairwise.cuh"
 #include "rnn.cuh"
+#include "screen.cuh"
 
 namespace cuhc {
 
@@ -52,6 +53,16 @@ std::atomic<int> gScreenMode{0};
 // Set by the batched path's autotuner for the duration of one call.
 thread_local int tScreenOverride = -1;
 int currentScreenMode() { return tScreenOverride >= 0 ? tScreenOverride : gScreenMode.load(); }
+thread_local ScreenShape tScreenShape;
+std::atomic<int> gLastShapeStages{0}, gLastShapeLead{0};
+ScreenShape currentScreenShape() { return tScreenShape; }
+void setScreenShape(ScreenShape shape) {
+  tScreenShape = shape;
+  if (shape.stages > 0) {
+    gLastShapeStages.store(shape.stages);
+    gLastShapeLead.store(shape.lead);
+  }
+}
 
 int pairwiseIntoMatrix(const float *points, int n, int d, int metricId, float p, float *out,
                        cudaStream_t s) {
@@ -368,6 +379,16 @@ int validateHdbscan(int n, int d, int minSamples, int coreMethod) {
 using namespace cuhc;
 
 extern "C" {
+
+// The pipeline shape (ring slots, copy lead) the shape tuner chose for the
+// latest screened k-NN pass of any thread (0, 0 before any). Diagnostic.
+int cuhc_screen_shape(int *stages, int *lead) {
+  if (!stages || !lead)
+    return cuhc::kErrorInvalidShape;
+  *stages = cuhc::gLastShapeStages.load();
+  *lead = cuhc::gLastShapeLead.load();
+  return 0;
+}
 
 int cuhc_pairwise_distances(const float *hostA, int nA, const float *hostB, int nB, int d,
                             int metricId, float p, float *hostOut) {

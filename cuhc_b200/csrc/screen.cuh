@@ -53,6 +53,7 @@
 // every later wait gives up at once, and the pass returns kErrorTimeout.
 #pragma once
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <type_traits>
@@ -450,14 +451,14 @@ __device__ __noinline__ void auditTile(unsigned long long *words, uint32_t taddr
 // on), so that the audit costs the normal kernel nothing.
 template <class Metric, class Weight, int KC, bool kKnn, bool kAudit>
 __global__ void __launch_bounds__(kThreads, 2)
-    screenKernel(PassParams p, Metric m, Weight w, float margin, int stages) {
+    screenKernel(PassParams p, Metric m, Weight w, float margin, int stages, int leadArg) {
   using L = ScreenLayout<KC>;
   const L layout{stages};
   constexpr int kPad = L::kPad;
   constexpr uint32_t kSbo = kPad * 32;
   constexpr int R = screenSlots(KC);
   const int S = stages;
-  const int lead = min(S - 1, screenLead(KC));
+  const int lead = leadArg;
   extern __shared__ __align__(128) float dyn[];
   __shared__ PassState sh;
   __shared__ ScreenSync ss;
@@ -1139,6 +1140,16 @@ __global__ void __launch_bounds__(kThreads, 2)
 // 2 never). Results are identical in every mode.
 int currentScreenMode();
 
+// Pipeline shape of a screened launch: ring slots and copy lead (0: the
+// defaults, the most slots that keep two blocks on an SM and screenLead).
+// Set per calling thread by the shape tuner (tunedScreenShape); a shape
+// changes time only, never a result.
+struct ScreenShape {
+  int stages = 0, lead = 0;
+};
+ScreenShape currentScreenShape();
+void setScreenShape(ScreenShape shape);
+
 template <class Metric> struct ScreenSupport {
   static constexpr bool value = false;
 };
@@ -1215,9 +1226,14 @@ int launchScreen(const PassParams &p, const Metric &m, const Weight &w, int kc,
     const float margin = std::is_same<Metric, CosineMetric>::value
                              ? screenMarginCosine(p.d, kc)
                              : screenMargin(p.d, kc);
-    const int stages = screenStagesFor(p.d, kKnn ? p.k : 0);
-    if (stages == 0)
+    const int maxStages = screenStagesFor(p.d, kKnn ? p.k : 0);
+    if (maxStages == 0)
       return kErrorInvalidAlgorithm;
+    const ScreenShape shape = currentScreenShape();
+    const int stages =
+        shape.stages > 0 ? std::max(kScreenMinStages, std::min(shape.stages, maxStages)) : maxStages;
+    const int lead = std::max(1, std::min(stages - 1, shape.lead > 0 ? shape.lead
+                                                                     : screenLead(kc)));
     const size_t dynBytes = screenDynamicBytes(p.d, kKnn ? p.k : 0, stages);
     auto misaligned = [](const void *ptr) { return ((uintptr_t)ptr & 15) != 0; };
     if (misaligned(p.tiled) || misaligned(p.order) || misaligned(p.component) ||
@@ -1228,7 +1244,7 @@ int launchScreen(const PassParams &p, const Metric &m, const Weight &w, int kc,
           cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dynBytes);
       if (e != cudaSuccess)
         return (int)e;
-      kernel<<<p.numTiles, kThreads, dynBytes, stream>>>(p, m, w, margin, stages);
+      kernel<<<p.numTiles, kThreads, dynBytes, stream>>>(p, m, w, margin, stages, lead);
       noteLaunch();
       return (int)cudaGetLastError();
     };

@@ -146,6 +146,10 @@ int cuhc_set_radius_model(const float *params, float offset);
 /* Since the last call (first `count` of: rows proposed, rows certified,
  * tiles of the capped passes, tiles of the fallback passes). */
 int cuhc_radius_stats(unsigned long long *out, int count);
+/* The pipeline shape (ring slots, copy lead) that the shape tuner chose for
+ * the latest screened k-NN pass (0, 0 before any). No counterpart in the
+ * reference: the tuner times candidate shapes once per (metric, d, k). */
+int cuhc_screen_shape(int *stages, int *lead);
 /* Up to maxRowsPerRound random rows per exact single-linkage round of points
  * (HOST, n x 16): features [rows][19], targets (log nearest other-component
  * weight); at most `capacity` rows written, *rows = rows found. */
