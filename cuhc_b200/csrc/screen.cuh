@@ -165,6 +165,61 @@ place:
   list[i] = key;
 }
 
+// k-NN, the row tile against itself (every list still empty): a bound on the
+// screened value of every pair that can enter the row's list, so that only
+// those pairs are rechecked instead of all 128. With T the k-th smallest
+// screened value D' over the tile's valid columns (bisected to within 2^-8 of
+// the value range, from above), the k columns of smallest D' all have exact
+// values s <= D' + delta <= T + delta (delta bounds s - D' for every pair of the
+// tile), so the row's k-th smallest exact value in the tile, and every pair
+// that can still enter its list, has D' <= s <= T + delta. +inf when the tile
+// holds fewer than k valid columns. Whole warp (tensor-memory loads).
+__device__ __forceinline__ float selfTileBound(uint32_t taddr, const int *cOrig, int firstCol,
+                                               int n, int k, float delta) {
+  const int lane = threadIdx.x & 31;
+  uint32_t valid[4];
+  int count = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    valid[q] = __ballot_sync(0xffffffffu,
+                             firstCol + q * 32 + lane < n && cOrig[q * 32 + lane] >= 0);
+    count += __popc(valid[q]);
+  }
+  if (count < k)
+    return INFINITY;
+  float lo = INFINITY, hi = -INFINITY;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    float v[32];
+    tmemLoad32(taddr + q * 32, v);
+#pragma unroll
+    for (int c = 0; c < 32; ++c)
+      if ((valid[q] >> c) & 1u) {
+        lo = fminf(lo, v[c]);
+        hi = fmaxf(hi, v[c]);
+      }
+  }
+  // Invariant: at least k valid values are <= hi.
+#pragma unroll 1
+  for (int step = 0; step < 8; ++step) {
+    const float mid = 0.5f * (lo + hi);
+    int below = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      float v[32];
+      tmemLoad32(taddr + q * 32, v);
+#pragma unroll
+      for (int c = 0; c < 32; ++c)
+        below += (((valid[q] >> c) & 1u) && v[c] <= mid) ? 1 : 0;
+    }
+    if (below >= k)
+      hi = mid;
+    else
+      lo = mid;
+  }
+  return hi + delta;
+}
+
 // Dynamic shared memory of a screened block with `stages` ring slots, in
 // floats from the base (every region 16-byte aligned).
 template <int KC> struct ScreenLayout {
@@ -464,6 +519,8 @@ __global__ void __launch_bounds__(kThreads, 2)
   __shared__ ScreenSync ss;
   // Bounding box of each consumer warp's valid rows (+inf/-inf when none).
   __shared__ float groupLow[4 * KC], groupHigh[4 * KC];
+  // k-NN: the largest centred squared norm of each consumer warp's valid rows.
+  __shared__ float groupNorm[4];
   float *sA = dyn + layout.sA();
   float *rawBase = dyn + layout.raw();
   int *metaBase = reinterpret_cast<int *>(dyn + layout.meta());
@@ -576,11 +633,27 @@ __global__ void __launch_bounds__(kThreads, 2)
   tcgenFenceAfter();
   const uint32_t tmem = ss.tmemBase;
   const bool oneHot = ss.oneHot != 0;
+  float myNorm = 0.0f; // k-NN: the row's centred squared norm
   if (consumer) {
     if constexpr (kCos)
       buildRowOperandCosine<KC>(sA, myRow, mySearch, myComp, ss, opA);
     else
       buildRowOperand<KC>(sA, centre, scale, myRow, mySearch, myComp, ss, opA);
+    if (kKnn) {
+      float nrm = 0.0f;
+#pragma unroll
+      for (int k = 0; k < KC; ++k) {
+        const float x = sA[k * kTile + myRow] - centre[k];
+        nrm = fmaf(x, x, nrm);
+      }
+      myNorm = myValid ? nrm : 0.0f;
+      float mx = myNorm;
+#pragma unroll
+      for (int off = 16; off > 0; off /= 2)
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      if (lane == 0)
+        groupNorm[warp] = mx;
+    }
 #pragma unroll
     for (int k = 0; k < KC; ++k) {
       float lo = mySearch ? sA[k * kTile + myRow] : INFINITY;
@@ -917,6 +990,16 @@ __global__ void __launch_bounds__(kThreads, 2)
           // its bound -- the candidate bits of both chunks, built from the
           // same registers (no second read of tensor memory).
           float Fs = F + kScreenAbsSlack;
+          if (kKnn && J == I && p.k <= kTile) {
+            // delta: 1.5 e (|x|^2 + |y|^2) bounds s - D' (the margin e is twice
+            // the error bound); twice that, with the tile's largest norm.
+            const float normMax = fmaxf(fmaxf(groupNorm[0], groupNorm[1]),
+                                        fmaxf(groupNorm[2], groupNorm[3]));
+            const float delta =
+                (kCos ? 2.0f * margin : 2.02f * margin * (myNorm + normMax)) + 0x1p-60f;
+            Fs = fminf(Fs, selfTileBound(taddr, cOrig, J * kTile, p.n, p.k, delta) +
+                               kScreenAbsSlack);
+          }
           uint32_t cand[4];
 #pragma unroll
           for (int half = 0; half < 2; ++half) {
