@@ -284,7 +284,8 @@ __device__ __forceinline__ void storeOperandRow(float *op, int row, const float 
         make_float4(val[4 * q], val[4 * q + 1], val[4 * q + 2], val[4 * q + 3]);
 }
 
-// Row operand of row tile point i: [x (KC), N hi, N lo, 1, 1, indicators].
+// Row operand of row tile point i: [-2 x (KC), N hi, N lo, 1, 1, indicators]
+// (the factor -2, exact, sits on the side built once per row tile).
 template <int KC>
 __device__ __forceinline__ void buildRowOperand(const float *sA, const float *centre, float scale,
                                                 int i, bool valid, int comp,
@@ -296,7 +297,7 @@ __device__ __forceinline__ void buildRowOperand(const float *sA, const float *ce
   for (int k = 0; k < KC; ++k) {
     const float x = sA[k * kTile + i] - centre[k];
     n = fmaf(x, x, n);
-    val[k] = toTf32(x);
+    val[k] = -2.0f * toTf32(x);
   }
   const float ns = n * scale, nh = toTf32(ns);
   val[KC] = nh;
@@ -310,10 +311,11 @@ __device__ __forceinline__ void buildRowOperand(const float *sA, const float *ce
   storeOperandRow<kPad>(opA, i, val);
 }
 
-// Column operand of staged point j: [-2 y (KC), 1, 1, N hi, N lo, indicators].
+// Column operand of staged point j: [y (KC), 1, 1, N hi, N lo, indicators];
+// the tile centre comes in registers.
 template <int KC>
 __device__ __forceinline__ void buildColumnOperand(const float *raw, const int *comp,
-                                                   const float *centre, float scale, int j,
+                                                   const float (&centre)[KC], float scale, int j,
                                                    bool oneHot, const ScreenSync &ss,
                                                    float *opB) {
   constexpr int kPad = screenKPad(KC), R = screenSlots(KC);
@@ -323,7 +325,7 @@ __device__ __forceinline__ void buildColumnOperand(const float *raw, const int *
   for (int k = 0; k < KC; ++k) {
     const float y = raw[k * kTile + j] - centre[k];
     n = fmaf(y, y, n);
-    val[k] = -2.0f * toTf32(y);
+    val[k] = toTf32(y);
   }
   const float ns = n * scale, nh = toTf32(ns);
   val[KC] = 1.0f;
@@ -348,7 +350,7 @@ __device__ __forceinline__ float unitScale(const float *x, int stride, int i) {
   return n > 0.0f ? rsqrtf(n) : 0.0f;
 }
 
-// Row operand of row tile point i (cosine): [x^ (KC), 1, 0, 0, 0, indicators].
+// Row operand of row tile point i (cosine): [-x^ (KC), 1, 0, 0, 0, indicators].
 template <int KC>
 __device__ __forceinline__ void buildRowOperandCosine(const float *sA, int i, bool valid, int comp,
                                                       const ScreenSync &ss, float *opA) {
@@ -357,7 +359,7 @@ __device__ __forceinline__ void buildRowOperandCosine(const float *sA, int i, bo
   const float r = unitScale<KC>(sA, kTile, i);
 #pragma unroll
   for (int k = 0; k < KC; ++k)
-    val[k] = toTf32(sA[k * kTile + i] * r);
+    val[k] = -toTf32(sA[k * kTile + i] * r);
   val[KC] = 1.0f;
   val[KC + 1] = 0.0f;
   val[KC + 2] = 0.0f;
@@ -369,7 +371,7 @@ __device__ __forceinline__ void buildRowOperandCosine(const float *sA, int i, bo
   storeOperandRow<kPad>(opA, i, val);
 }
 
-// Column operand of staged point j (cosine): [-y^ (KC), c, 0, 0, 0,
+// Column operand of staged point j (cosine): [y^ (KC), c, 0, 0, 0,
 // indicators], c = 1 - e rounded down to TF32.
 template <int KC>
 __device__ __forceinline__ void buildColumnOperandCosine(const float *raw, const int *comp,
@@ -380,7 +382,7 @@ __device__ __forceinline__ void buildColumnOperandCosine(const float *raw, const
   const float r = unitScale<KC>(raw, kTile, j);
 #pragma unroll
   for (int k = 0; k < KC; ++k)
-    val[k] = -toTf32(raw[k * kTile + j] * r);
+    val[k] = toTf32(raw[k * kTile + j] * r);
   val[KC] = c;
   val[KC + 1] = 0.0f;
   val[KC + 2] = 0.0f;
@@ -676,6 +678,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   unsigned long long rowBest = settled ? kEmptyKey : mySeed;
   int tie = 0; // k-NN: a point outside the row's list ties its k-th value
   float F = -INFINITY;
+  float rowThr = INFINITY; // the row's weight threshold at the last refresh
   auto refresh = [&](unsigned int cb) -> float {
     float thr;
     if (kKnn) {
@@ -696,6 +699,7 @@ __global__ void __launch_bounds__(kThreads, 2)
               ? m.screenBound(w.distBound(thr, myVal))
               : -INFINITY;
     }
+    rowThr = thr;
     return F == -INFINITY ? -INFINITY : thr;
   };
   // Publishes the warp's largest threshold (for the block's candidate cut),
@@ -938,6 +942,10 @@ __global__ void __launch_bounds__(kThreads, 2)
     } else if (!consumer) {
       // ---- builders: warps 4..5, columns j and j + 64 ----
       const int j = tid - kTile;
+      float cen[KC];
+#pragma unroll
+      for (int k = 0; k < KC; ++k)
+        cen[k] = centre[k];
       while (true) {
         const int s = t & 1;
         // The operand buffer of slot s is free once the MMA of ordinal t - 2
@@ -955,7 +963,7 @@ __global__ void __launch_bounds__(kThreads, 2)
             if constexpr (kCos)
               buildColumnOperandCosine<KC>(raw, comp, cosC, q, oneHot, ss, b);
             else
-              buildColumnOperand<KC>(raw, comp, centre, scale, q, oneHot, ss, b);
+              buildColumnOperand<KC>(raw, comp, cen, scale, q, oneHot, ss, b);
         }
         fenceProxyAsync();
         __syncwarp();
@@ -990,6 +998,24 @@ __global__ void __launch_bounds__(kThreads, 2)
           // its bound -- the candidate bits of both chunks, built from the
           // same registers (no second read of tensor memory).
           float Fs = F + kScreenAbsSlack;
+          if constexpr (std::is_same<Weight, WardWeight>::value) {
+            // Ward: F assumes the lightest partner (size 1); the column tile's
+            // smallest cluster size s_min tightens it, since 2 si sj / (si + sj)
+            // grows with sj: a pair weighs <= thr only if its squared distance
+            // is <= thr (1/si + 1/s_min) / 2 (rounded up, as distBound).
+            float sMin = INFINITY;
+#pragma unroll
+            for (int c = lane; c < kTile; c += 32)
+              if (J * kTile + c < p.n && cOrig[c] >= 0)
+                sMin = fminf(sMin, cVal[c]);
+#pragma unroll
+            for (int off = 16; off > 0; off /= 2)
+              sMin = fminf(sMin, __shfl_xor_sync(0xffffffffu, sMin, off));
+            if (F > -INFINITY && rowThr < INFINITY && sMin < INFINITY)
+              Fs = fminf(Fs, m.screenBound(__fmul_ru(
+                                 rowThr, (1.0f / myVal + 1.0f / sMin) * 0.5f * 1.00001f)) +
+                                 kScreenAbsSlack);
+          }
           if (kKnn && J == I && p.k <= kTile) {
             // delta: 1.5 e (|x|^2 + |y|^2) bounds s - D' (the margin e is twice
             // the error bound); twice that, with the tile's largest norm.
