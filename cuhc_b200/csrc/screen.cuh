@@ -984,10 +984,6 @@ __global__ void __launch_bounds__(kThreads, 2)
         const int r = tSlot;
         bool thrChanged = false;
         if (entry >= 0) {
-          // The component best for this tile's refresh, loaded before the
-          // accumulator is read so that its L2 latency overlaps the reads (a
-          // value one tile old is only larger: still a valid bound).
-          const unsigned int cbNow = compSlot ? __ldcg(compSlot) : 0xffffffffu;
           const int J = entry & ~kPureColumnTile;
           const bool colPure = (entry & kPureColumnTile) != 0;
           const float *raw = rawBase + r * L::rawFloats;
@@ -1149,7 +1145,7 @@ __global__ void __launch_bounds__(kThreads, 2)
           // component's best (found by other blocks): refresh then, and every
           // eighth tile for the latter.
           if (__any_sync(0xffffffffu, dirty) || (computed & 7) == 7) {
-            publish(refresh(cbNow));
+            publish(refresh(compSlot ? __ldcg(compSlot) : 0xffffffffu));
             dirty = false;
             thrChanged = true;
           }
