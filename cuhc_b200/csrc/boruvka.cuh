@@ -388,7 +388,7 @@ int boruvkaMst(SpatialIndex &index, const Metric &metric, const Weight &weight, 
     p.singletons = first;
     p.radius = nullptr;
     // Heaviest row tiles first: by the last pass's work (boxes before any).
-    CUHC_TRY(rs, index.orderTiles(!index.tileWorkValid));
+    CUHC_TRY(rs, index.orderTiles(!index.tileWorkValid, true));
     p.tileOrder = index.tileOrder.get();
     p.tileWork = index.tileWork.get();
     if (useRadius || logRows)

@@ -605,17 +605,22 @@ __global__ void tileKeysFromBoxes(const float *__restrict__ low, const float *__
 }
 
 __global__ void tileKeysFromWork(const unsigned int *__restrict__ work, int numTiles,
+                                 const int *__restrict__ nodePure,
+                                 const int *__restrict__ leafOfTile,
                                  unsigned int *__restrict__ keys, int *__restrict__ iota) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= numTiles)
     return;
-  keys[t] = work[t];
+  const unsigned int w = min(work[t], 0x7fffffffu);
+  // Row tiles holding several components first (with nodePure): their rows
+  // sit on component boundaries, where the components' lightest edges are.
+  keys[t] = nodePure && nodePure[leafOfTile[t]] < 0 ? w | 0x80000000u : w;
   iota[t] = t;
 }
 
 } // namespace
 
-int SpatialIndex::orderTiles(bool fromBoxes) {
+int SpatialIndex::orderTiles(bool fromBoxes, bool impureFirst) {
   StatusChain st;
   if (!tileOrder.get()) {
     CUHC_TRY(st, tileWork.allocate(numTiles, stream));
@@ -637,7 +642,8 @@ int SpatialIndex::orderTiles(bool fromBoxes) {
         tileIota.get());
   else
     tileKeysFromWork<<<blocksFor(numTiles, 256), 256, 0, stream>>>(
-        tileWork.get(), numTiles, tileKeys.get(), tileIota.get());
+        tileWork.get(), numTiles, impureFirst ? nodePure.get() : nullptr, leafOfTile.get(),
+        tileKeys.get(), tileIota.get());
   noteLaunch();
   CUHC_TRY(st, cudaGetLastError());
   CUHC_TRY(st, cub::DeviceRadixSort::SortPairsDescending(

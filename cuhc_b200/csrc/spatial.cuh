@@ -99,7 +99,9 @@ struct SpatialIndex {
   // tileOrder <- row tiles by decreasing tileWork (fromBoxes: by decreasing
   // leaf box log-volume, the estimate before any pass has run). Enqueued on
   // the index stream with no host work (buffers are allocated on first use).
-  int orderTiles(bool fromBoxes);
+  // impureFirst: row tiles whose points span several components (nodePure
+  // of the round) go before the others, each group heaviest first.
+  int orderTiles(bool fromBoxes, bool impureFirst = false);
 };
 
 } // namespace cuhc
