@@ -445,7 +445,8 @@ def run_hdbscan(args, rank, world, local_rank):
 
     # End to end through the host API (pinned buffers, copies included).
     host_step()
-    e2e = float(np.mean(timed(host_step, args.steps)))
+    e2e_times = timed(host_step, args.steps)
+    e2e = float(np.mean(e2e_times))
     identical_e2e = bool(np.array_equal(tree_pin.numpy(), screened_tree))
 
     # One audited step: every evaluated pair's screened bound against FP32 / FP64.
@@ -478,6 +479,8 @@ def run_hdbscan(args, rank, world, local_rank):
             "e2e": {"value": round(e2e, 4), "unit": UNIT, "h2d_bytes_per_step": int(X.nbytes),
                     "d2h_bytes_per_step": int((n - 1) * 4 * 8 + n * 4)},
             "gpu_launches": int(launches),
+            "step_ms": {"device": [round(x * 1e3, 2) for x in times],
+                        "e2e": [round(x * 1e3, 2) for x in e2e_times]},
             "roofline": roofline(kt, d, fp32, clock),
             "plain_fp32": {"value": None if np.isnan(plain) else round(plain, 4), "unit": UNIT,
                            "speedup_screened": None if np.isnan(plain) else
