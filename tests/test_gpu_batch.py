@@ -59,3 +59,16 @@ def test_repeat_is_identical():
     for (Za, ca), (Zb, cb) in zip(a, b):
         np.testing.assert_array_equal(Za, Zb)
         np.testing.assert_array_equal(ca, cb)
+
+
+def test_cosine_batch():
+    """Cosine, which runs on the tensor-core screen: every batched tree equals
+    its own call's (zero points and antiparallel copies included)."""
+    instances = []
+    for n in (3, 129, 700, 2000):
+        X = blobs(n, 16, noise=0.1, seed=n)
+        if n >= 129:
+            X[:4] = 0.0
+            X[4:20] = -X[20:36]
+        instances.append(X)
+    _check(instances, [0, 5, 0, 9], metric="cosine")
